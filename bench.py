@@ -1,0 +1,330 @@
+"""Benchmark: CG time-to-solution for the fat+Naik staggered even-odd system.
+
+Workload (one step = one solve): 32^4 lattice, fat+Naik links (fat =
+0.8*SU(3) + N(0, 0.2^2) entries, long = SU(3), phases folded in), mass
+0.01, Gaussian even-site source, solve stagD2ee(m^2) y = b (QEX's solveEE)
+to a true FP64 relative residual of 1e-10 (r2req = 1e-20).  `value` is the
+time to solution of the fastest solver configuration on device-resident
+inputs; the plain FP64 CG time is reported beside it.  `e2e` is the same
+solve through the C ABI with host (QEX-layout) buffers, copies included.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--dims 32,32,32,32]
+
+With N > 1 (torchrun) every rank solves its own replica (the solve does not
+shard across GPUs here); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MASS = 0.01
+R2REQ = 1e-20
+# FP64 CG iteration count of this workload at 32^4 (used only by the CPU
+# reference arm to turn its per-iteration time into a time to solution)
+FP64_ITERS_32 = None
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_inputs(dims, rank):
+    from qex_b200 import fields as F
+    g = F.fat_naik_links(dims, 21 + 1000 * rank)
+    b = F.even_source(dims, 31 + 1000 * rank)
+    return g, b
+
+
+def cpu_sample(dims, g, b, iters, fp64_iters):
+    """Oracle (C, OpenMP, all host threads) FP64 CG sampled for `iters`
+    iterations on the full workload; extrapolated to fp64_iters iterations."""
+    from oracle import oracle as O
+    o = O.Oracle(dims, g)
+    y = o.vec()
+    o.cg(0, y, b, MASS * MASS, R2REQ, maxits=1)  # warm
+    t0 = time.perf_counter()
+    its, _ = o.cg(0, y, b, MASS * MASS, R2REQ, maxits=iters)
+    dt = time.perf_counter() - t0
+    per_it = dt / max(its, 1)
+    return per_it * fp64_iters, per_it, its, dt, O.num_threads()
+
+
+def run_reference(args, dims):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    g, b = make_inputs(dims, 0)
+    its_full = args.ref_iters
+    vals = []
+    sample = None
+    for step in range(args.warmup + args.steps):
+        v, per_it, its, dt, cores = cpu_sample(dims, g, b, args.cpu_iters, its_full)
+        if step >= args.warmup:
+            vals.append(v)
+        sample = (f"{its} FP64 CG iterations of the oracle (C/OpenMP restatement of QEX cg.nim + "
+                  f"stagD2ee) on the full {dims} workload, {per_it*1e3:.1f} ms/iteration, "
+                  f"extrapolated to {its_full} iterations")
+    val = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": val * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded numpy: warmSU(0.3) links, Gaussian source)",
+            "config": config_dict(dims),
+            "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "CG time-to-solution, FP64 true residual 1e-10, fat+Naik even-odd, m=0.01"
+
+
+def config_dict(dims):
+    return {"workload": f"fat+Naik staggered even-odd CG, {'x'.join(map(str, dims))}, m={MASS}, "
+                        f"Gaussian even source, true r2 <= 1e-20 |b|^2",
+            "lattice": list(dims), "mass": MASS, "r2req": R2REQ,
+            "l2": "inputs larger than L2 (links 1.2 GB FP64), no flush needed"}
+
+
+def timed_solves(s, yd, bd, sp_kw, steps, torch):
+    from qex_b200 import stag as S
+    times, launches, iters, sps = [], 0, [], []
+    for _ in range(steps):
+        sp = S.SolverParams(r2req=R2REQ, **sp_kw)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.solveEE(yd, bd, MASS, sp)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+        launches += sp.kernel_launches
+        iters.append(sp.iterations)
+        sps.append(sp)
+    return times, launches, iters, sps
+
+
+def run_ours(args, dims):
+    import torch
+
+    from qex_b200 import fields as F
+    from qex_b200 import stag as S
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    S.init(local)
+    S.set_stream(torch.cuda.current_stream().cuda_stream)
+    g, b = make_inputs(dims, rank)
+    V = F.volume(dims)
+    nh = V // 2
+    lay = S.Layout(dims, device=local)
+    s = S.Staggered(lay, S.to_device_links(g))
+    bd = S.to_device_vector(b)
+    yd = torch.zeros((3, V), dtype=torch.complex128, device="cuda")
+
+    configs = [("fp64", {"sloppySolve": 0})]
+    results = {}
+    for name, kw in configs:
+        # warm-up
+        timed_solves(s, yd, bd, kw, args.warmup, torch)
+        barrier(ws)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            times, launches, iters, sps = timed_solves(s, yd, bd, kw, args.steps, torch)
+        torch.cuda.synchronize()
+        barrier(ws)
+        t = max_over_ranks(float(np.mean(times)), ws)
+        # true residual of the last solution (FP64, through the library)
+        ay = torch.zeros_like(yd)
+        s.stagD2ee(ay, yd, MASS * MASS)
+        rr = ((ay[:, :nh] - bd[:, :nh]).abs() ** 2).sum().item() / (bd[:, :nh].abs() ** 2).sum().item()
+        results[name] = {"time_s": t, "iterations": iters[-1], "true_r2": rr,
+                         "outer": sps[-1].outer_iterations, "reliable_updates": sps[-1].reliable_updates,
+                         "launches": launches, "clocks": clk.summary()}
+    best = min(results, key=lambda k: results[k]["time_s"])
+    value = results[best]["time_s"]
+
+    # roofline of the dominant kernel: the FP64 fat+Naik Schur half-sweeps
+    xd = torch.randn((3, V), dtype=torch.complex128, device="cuda")
+    rd = torch.zeros_like(xd)
+    for _ in range(3):
+        s.stagD2ee(rd, xd, MASS * MASS)
+    nrep = 20
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(nrep):
+        s.stagD2ee(rd, xd, MASS * MASS)
+    e1.record()
+    torch.cuda.synchronize()
+    per_call = e0.elapsed_time(e1) * 1e-3 / nrep
+    bytes_per_site = 2400 + 2448  # two fat+Naik FP64 half sweeps, see DESIGN.md
+    alg = bytes_per_site * nh
+    achieved = alg / per_call / 1e9
+    peak, peak_kind = measured_peaks()
+    roof = {"kernel": "dslash64_kernel<8,*> x2 (stagD2ee, FP64 fat+Naik)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+            "traffic": None, "bytes_per_even_site": bytes_per_site,
+            "gflops": round((2 * 1146) * nh / per_call / 1e9, 1)}
+
+    # e2e: the same solve through the C ABI with host buffers
+    bh = np.ascontiguousarray(b)
+    yh = np.zeros_like(bh)
+    kw = configs[[c[0] for c in configs].index(best)][1]
+    e2e_times = []
+    for i in range(max(1, args.steps)):
+        sp = S.SolverParams(r2req=R2REQ, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.solveEE(yh, bh, MASS, sp)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e = max_over_ranks(float(np.mean(e2e_times)), ws)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu:
+            its64 = results["fp64"]["iterations"]
+            v, per_it, its, dt, cores = cpu_sample(dims, g, b, args.cpu_iters, its64)
+            cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port",
+                   "sample": f"{its} FP64 CG iterations of the oracle on the full workload "
+                             f"({per_it*1e3:.1f} ms/iteration, {dt:.1f} s), extrapolated to the "
+                             f"{its64} iterations the FP64 solve takes"}
+        line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if best == "fp64" else best,
+                "data": "synthetic (seeded numpy: warmSU(0.3) links, Gaussian source)",
+                "config": config_dict(dims), "solver": best,
+                "solvers": {k: {kk: vv for kk, vv in v.items() if kk != "clocks"} for k, v in results.items()},
+                "fp64_time_s": results["fp64"]["time_s"],
+                "speedup_vs_fp64": results["fp64"]["time_s"] / value,
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(bh.nbytes),
+                        "d2h_bytes_per_step": int(yh.nbytes)},
+                "clocks": results[best]["clocks"],
+                "gpu_launches": int(results[best]["launches"])}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--dims", default="32,32,32,32")
+    ap.add_argument("--cpu-iters", type=int, default=40)
+    ap.add_argument("--ref-iters", type=int, default=0,
+                    help="FP64 iterations to extrapolate the reference arm to")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    dims = tuple(int(v) for v in args.dims.split(","))
+    if args.impl == "reference":
+        if args.ref_iters <= 0:
+            args.ref_iters = FP64_ITERS_32 or 1
+        run_reference(args, dims)
+    else:
+        run_ours(args, dims)
+
+
+if __name__ == "__main__":
+    main()

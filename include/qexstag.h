@@ -1,0 +1,212 @@
+/*
+ * qexstag.h -- C ABI of the B200 (sm_100a) staggered-fermion library.
+ *
+ * This is the boundary a QEX (Nim) host calls through {.importc, dynlib.},
+ * in the same way QEX already calls QUDA's MILC interface
+ * (src/quda/quda_milc_interface.nim:289-295, called from
+ * src/quda/qudaWrapperImpl.nim:252-255).  Every entry point takes plain C
+ * types; none takes a C++ or torch type.
+ *
+ * Conventions
+ *  - Every function returns an int status: QEXSTAG_OK (0); a positive value
+ *    when a solver stopped without reaching its target (the result is still
+ *    written); a negative QEXSTAG_ERR_* on error.  qexstag_last_error()
+ *    returns a text description of the last error on the calling thread.
+ *  - Lattice: dims[4] = {L0,L1,L2,L3}, each even and >= 4.  Sites are
+ *    numbered as QEX numbers them with SIMD width 1 on one rank
+ *    (src/layout/qlayout.nim:108-136):
+ *      lex = x0 + L0*(x1 + L1*(x2 + L2*x3)),
+ *      idx = (lex + (x0+x1+x2+x3 odd ? V : 0)) / 2,
+ *    so even sites are [0, V/2) and odd sites [V/2, V).
+ *  - Host fields (QEXSTAG_MEM_HOST) are in that order, array-of-structs:
+ *      colour vector: double[V][3][2]              (re, im)
+ *      link field k:  double[nlinks][V][3][3][2]   (row-major 3x3)
+ *  - Device fields (QEXSTAG_MEM_DEVICE) are CUDA device pointers in the
+ *    library's structure-of-arrays layout, which coalesces on the GPU:
+ *      colour vector: double2[3][V]   (colour-major, then site index)
+ *    Even-parity-only vectors may instead be given as double2[3][V/2]
+ *    where an entry point says so.
+ *  - Link lists follow QEX's Staggered.g: nlinks == 4 is naive staggered
+ *    (link k = direction k, one hop); nlinks == 8 is fat+Naik interleaved as
+ *    newStag3 builds it (src/physics/stagD.nim:40-51, 603-615): link 2*mu is
+ *    the fat link (hop 1), link 2*mu+1 the long link (hop 3).  Links must
+ *    already carry the staggered phases and boundary signs (QEX's
+ *    setBC + stagPhase, src/physics/stagD.nim:106-114, 560-571).
+ *  - Calls on one handle are not reentrant; separate handles and separate
+ *    devices may be used from separate threads.  Work is issued on the
+ *    stream set by qexstag_set_stream (default: the legacy default stream).
+ */
+#ifndef QEXSTAG_H
+#define QEXSTAG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define QEXSTAG_OK 0
+#define QEXSTAG_NOT_CONVERGED 1
+#define QEXSTAG_ERR_ARG (-1)
+#define QEXSTAG_ERR_CUDA (-2)
+#define QEXSTAG_ERR_NAN (-3)
+#define QEXSTAG_ERR_TIMEOUT (-4)
+#define QEXSTAG_ERR_ALLOC (-5)
+#define QEXSTAG_ERR_STATE (-6)
+
+/* where field pointers live */
+#define QEXSTAG_MEM_HOST 0
+#define QEXSTAG_MEM_DEVICE 1
+
+/* parities / subsets, as QEX's "even", "odd", "all" */
+#define QEXSTAG_EVEN 0
+#define QEXSTAG_ODD 1
+#define QEXSTAG_ALL 2
+
+/* inner-solver precision, QEX's SloppyType (src/solvers/solverBase.nim:8-9) */
+#define QEXSTAG_SLOPPY_NONE 0
+#define QEXSTAG_SLOPPY_SINGLE 1
+#define QEXSTAG_SLOPPY_HALF 2
+
+typedef struct qexstag_layout_s qexstag_layout;
+typedef struct qexstag_links_s qexstag_links;
+
+/* Solver inputs: the input half of QEX's SolverParams
+   (src/solvers/solverBase.nim:10-17).  r2req is the squared relative
+   residual, |b - A x|^2 <= r2req |b|^2 (src/solvers/cg.nim:155). */
+typedef struct {
+  double r2req;
+  int maxits;
+  int sloppy;          /* QEXSTAG_SLOPPY_* */
+  double delta;        /* reliable-update threshold for sloppy solves (0: 0.1) */
+  int verbosity;
+  int use_prev_soln;   /* solve(): start from the x passed in */
+  int reserved[6];
+} qexstag_solver_params;
+
+/* Solver outputs: the output half of QEX's SolverParams
+   (src/solvers/solverBase.nim:18-28). */
+typedef struct {
+  int calls;
+  int iterations;        /* Krylov iterations, all precisions */
+  int outer_iterations;  /* defect-correction / refinement passes */
+  int reliable_updates;
+  double seconds;        /* device time of the call */
+  double flops;          /* QEX's count, (nlinks*4*72+60)*nEven per iteration */
+  double r2;             /* final true |b - A x|^2 / |b|^2 (FP64) */
+  long long kernel_launches;  /* library kernels launched by the call */
+} qexstag_solver_stats;
+
+/* ---- runtime ---- */
+
+/* Select the CUDA device for the calling thread and set the library up on
+   it.  Replaces qexInit's device part; QUDA's initQuda analogue. */
+int qexstag_init(int device);
+/* Free every handle-independent resource on the current device. */
+int qexstag_finalize(void);
+/* Issue subsequent work on this cudaStream_t (NULL: legacy default). */
+int qexstag_set_stream(void *stream);
+/* Text of the last error on the calling thread (never NULL). */
+const char *qexstag_last_error(void);
+/* Block until all work issued by the library on its stream is done. */
+int qexstag_synchronize(void);
+
+/* ---- layout (src/layout/qlayout.nim, src/layout/shiftX.nim) ---- */
+
+/* Build the V=1 checkerboard layout for dims (newLayout with SIMD width 1,
+   src/layout/layoutX.nim:71-180). */
+int qexstag_layout_create(const int dims[4], qexstag_layout **out);
+int qexstag_layout_destroy(qexstag_layout *l);
+/* Site index of coordinates x (qlayout.nim:108-136, layoutIndexQ). */
+int qexstag_layout_index(const qexstag_layout *l, const int x[4], int64_t *idx);
+/* Neighbour table of ShiftB(mu, len, subset) (src/layout/shifts.nim:18-44,
+   src/layout/qshifts.nim:187-223): out_host[i] = index of x(i) + len*mu for
+   each destination site i of the subset, in subset order.  Computed on the
+   GPU with the index arithmetic the kernels use, then copied to host. */
+int qexstag_layout_shift_table(const qexstag_layout *l, int mu, int len, int subset,
+                               int32_t *out_host);
+
+/* ---- links (Staggered.g, src/physics/stagD.nim:68-86, 573-615) ---- */
+
+/* Upload a link list and build every precision the solvers use: FP64,
+   FP32 and FP16 copies, and 12-real (two-row) long links when the long
+   links are long_coeff times a phase times an SU(3) matrix to FP32 rounding
+   (checked here; otherwise long links keep all 18 reals).  links points to
+   nlinks*V*18 doubles in the host layout (mem == QEXSTAG_MEM_HOST) or to
+   double2[nlinks][9][V] on the device (mem == QEXSTAG_MEM_DEVICE).  The
+   handle keeps a pointer to l. */
+int qexstag_links_create(qexstag_layout *l, int nlinks, const double *links, int mem,
+                         double long_coeff, qexstag_links **out);
+int qexstag_links_destroy(qexstag_links *g);
+/* 1 when the handle uses 12-real long links in its reduced precisions. */
+int qexstag_links_recon12(const qexstag_links *g);
+
+/* ---- Dslash (src/physics/stagD.nim) ---- */
+
+/* stagD2 (stagD.nim:383-448): on subset (EVEN or ODD)
+     r = a*r + b*x + sum_k [U_k(s) x(s+d_k) - U_k(s-d_k)^dagger x(s-d_k)]. */
+int qexstag_stagD2(qexstag_links *g, int subset, double *r, const double *x, double a,
+                   double b, int mem);
+/* stagD (stagD.nim:459-462): r = a*r + m*x + (sc/2)(2D)x on subset
+   (EVEN, ODD or ALL). */
+int qexstag_stagD(qexstag_links *g, int subset, double *r, const double *x, double m,
+                  double sc, double a, int mem);
+/* D and Ddag (stagD.nim:617-622): r = m x +- (1/2)(2D) x on all sites. */
+int qexstag_D(qexstag_links *g, double *r, const double *x, double m, int mem);
+int qexstag_Ddag(qexstag_links *g, double *r, const double *x, double m, int mem);
+/* stagD2ee / stagD2oo (stagD.nim:485-520): on one parity p,
+   r_p = 4 m2 x_p - (2D)_pq (2D)_qp x_p.  Full-lattice fields. */
+int qexstag_stagD2ee(qexstag_links *g, double *r, const double *x, double m2, int mem);
+int qexstag_stagD2oo(qexstag_links *g, double *r, const double *x, double m2, int mem);
+
+/* ---- solvers (src/physics/stagSolve.nim, src/solvers/cg.nim, cgm.nim) ---- */
+
+/* solveEE / solveOO (stagSolve.nim:330-429): solve stagD2xx(m^2) r = x on
+   the parity with FP64 defect correction around CG.  p->sloppy selects the
+   inner precision (NONE: FP64 CG; SINGLE/HALF: FP32/FP16 reliable-update
+   CG).  r is overwritten (QEX zeroes it). Full-lattice fields. */
+int qexstag_solveEE(qexstag_links *g, double *r, const double *x, double m,
+                    const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
+int qexstag_solveOO(qexstag_links *g, double *r, const double *x, double m,
+                    const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
+/* solve (stagSolve.nim:469-557): D(m) x = b on the full lattice with
+   even-odd preconditioning and reconstruction (solveInner). */
+int qexstag_solve(qexstag_links *g, double *x, const double *b, double m,
+                  const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
+/* Multi-mass solve (stagSolve.nim:560-668): D(ms[k]) xs[k] = b for
+   k = 0..nmass-1 from multi-shift CG with shifts 4(ms[k]^2 - ms[0]^2). */
+int qexstag_solve_multishift(qexstag_links *g, int nmass, double *const *xs,
+                             const double *b, const double *ms,
+                             const qexstag_solver_params *p, qexstag_solver_stats *st,
+                             int mem);
+/* Shifted systems on even sites for rational terms and several right-hand
+   sides: (A + sigma[k]) y[j][k] = b[j], A = stagD2ee(m^2), for
+   j < nrhs, k < nshift, with one multi-shift CG per batch of right-hand
+   sides (links read once per site for all of them; cgm.nim:68-246), then,
+   for p->sloppy != NONE, FP64 refinement of each (j,k) to p->r2req.
+   b: nrhs pointers to full-lattice fields; y: nrhs*nshift pointers,
+   y[j*nshift+k].  r2_out (optional): nrhs*nshift final true |res|^2/|b|^2. */
+int qexstag_cgm_ee(qexstag_links *g, double m, int nshift, const double *sigma, int nrhs,
+                   const double *const *b, double *const *y,
+                   const qexstag_solver_params *p, qexstag_solver_stats *st,
+                   double *r2_out, int mem);
+
+/* ---- HMC force (src/hmc/hmcAction.nim:669-790, 851-885) ---- */
+
+/* stagForceSolve followed by fermForce without smearing: solves
+   stagD2ee(m^2) y = phi_e, psi = (4y, (2D)_oe 4y), then for every link k
+   f_k(x) = projectTAH(s(x) psi(x) psi(x + d_k)^dagger U_k(x)^dagger),
+   s = +1 on even and -1 on odd sites.  f: nlinks*V*18 doubles (host layout)
+   or double2[nlinks][9][V] (device).  This is the f QEX passes to
+   addForce(gf, 0.25*dtau, f). */
+int qexstag_force(qexstag_links *g, double *f, const double *phi, double m,
+                  const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
+/* fermForce alone for a given psi (full lattice). */
+int qexstag_ferm_force(qexstag_links *g, double *f, const double *psi, int mem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QEXSTAG_H */

@@ -1,0 +1,196 @@
+"""ctypes wrapper of the CPU oracle (qexstag_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, the smoke check and the CPU
+baseline leg of bench.py, as the checker.  PARITY UNPINNED: see the header
+of qexstag_oracle.c.
+
+Fields use the QEX V=1 host layout: complex128 (V, 3) colour vectors and
+(nlinks, V, 3, 3) link lists.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    src = HERE / "qexstag_oracle.c"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        l = C.CDLL(str(LIB))
+        P, D, I = C.c_void_p, C.c_double, C.c_int
+        DP = C.POINTER(C.c_double)
+        sig = {
+            "or_index": (C.c_long, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "or_coords": (None, [C.POINTER(C.c_int), P]),
+            "or_shift_table": (None, [C.POINTER(C.c_int), I, I, I, P]),
+            "or_ctx_create": (P, [C.POINTER(C.c_int), I, P]),
+            "or_ctx_set_links": (None, [P, P]),
+            "or_ctx_destroy": (None, [P]),
+            "or_stag_eta": (I, [I, C.POINTER(C.c_int)]),
+            "or_apply_phases": (None, [C.POINTER(C.c_int), I, P]),
+            "or_stagD2": (None, [P, I, P, P, D, D]),
+            "or_stagD": (None, [P, I, P, P, D, D, D]),
+            "or_D": (None, [P, P, P, D]),
+            "or_Ddag": (None, [P, P, P, D]),
+            "or_stagD2ee": (None, [P, P, P, D]),
+            "or_stagD2oo": (None, [P, P, P, D]),
+            "or_stagD2ee_par": (None, [P, I, P, P, D]),
+            "or_norm2": (D, [P, I, P]),
+            "or_redot": (D, [P, I, P, P]),
+            "or_cg_xx": (I, [P, I, P, P, D, D, I, DP]),
+            "or_solveXX": (I, [P, I, P, P, D, D, I, DP]),
+            "or_eoReconstruct": (None, [P, P, P, D]),
+            "or_solve": (I, [P, P, P, D, D, I, DP]),
+            "or_cgm_xx": (I, [P, I, I, C.POINTER(C.c_void_p), DP, P, D, D, I, DP]),
+            "or_solve_multishift": (I, [P, I, C.POINTER(C.c_void_p), P, DP, D, I, DP]),
+            "or_project_tah": (None, [P, P]),
+            "or_force_solve": (I, [P, P, P, D, D, I, DP]),
+            "or_ferm_force": (None, [P, P, P]),
+            "or_force": (I, [P, P, P, D, D, I, DP]),
+            "or_num_threads": (I, []),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return C.c_void_p(a.ctypes.data)
+
+
+def _dims(dims):
+    return (C.c_int * 4)(*[int(d) for d in dims])
+
+
+def index(dims, x) -> int:
+    return lib().or_index(_dims(dims), (C.c_int * 4)(*[int(v) for v in x]))
+
+
+def shift_table(dims, mu, length, parity) -> np.ndarray:
+    V = int(np.prod(dims))
+    n = V if parity == 2 else V // 2
+    out = np.empty(n, dtype=np.int32)
+    lib().or_shift_table(_dims(dims), mu, length, parity, _p(out))
+    return out
+
+
+def apply_phases(dims, links: np.ndarray) -> np.ndarray:
+    out = np.ascontiguousarray(links.copy())
+    lib().or_apply_phases(_dims(dims), out.shape[0], _p(out))
+    return out
+
+
+def project_tah(m: np.ndarray) -> np.ndarray:
+    m = np.ascontiguousarray(m, dtype=np.complex128)
+    out = np.empty_like(m)
+    lib().or_project_tah(_p(out), _p(m))
+    return out
+
+
+class Oracle:
+    """The oracle's operator on one lattice and link list."""
+
+    def __init__(self, dims, links: np.ndarray):
+        self.dims = tuple(int(d) for d in dims)
+        self.V = int(np.prod(self.dims))
+        self.links = np.ascontiguousarray(links, dtype=np.complex128)
+        assert self.links.shape[1:] == (self.V, 3, 3)
+        self.nlinks = self.links.shape[0]
+        self.ctx = lib().or_ctx_create(_dims(self.dims), self.nlinks, _p(self.links))
+
+    def __del__(self):
+        if getattr(self, "ctx", None):
+            lib().or_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def vec(self) -> np.ndarray:
+        return np.zeros((self.V, 3), dtype=np.complex128)
+
+    def stagD2(self, parity, r, x, a, b):
+        lib().or_stagD2(self.ctx, parity, _p(r), _p(x), a, b)
+
+    def stagD(self, parity, r, x, m, sc=1.0, a=0.0):
+        lib().or_stagD(self.ctx, parity, _p(r), _p(x), m, sc, a)
+
+    def D(self, r, x, m):
+        lib().or_D(self.ctx, _p(r), _p(x), m)
+
+    def Ddag(self, r, x, m):
+        lib().or_Ddag(self.ctx, _p(r), _p(x), m)
+
+    def stagD2ee(self, r, x, m2):
+        lib().or_stagD2ee(self.ctx, _p(r), _p(x), m2)
+
+    def stagD2oo(self, r, x, m2):
+        lib().or_stagD2oo(self.ctx, _p(r), _p(x), m2)
+
+    def norm2(self, parity, x) -> float:
+        return lib().or_norm2(self.ctx, parity, _p(x))
+
+    def cg(self, parity, x, b, m2, r2req, maxits=100000):
+        r2 = C.c_double()
+        its = lib().or_cg_xx(self.ctx, parity, _p(x), _p(b), m2, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+    def solveXX(self, parity, r, x, m, r2req, maxits=100000):
+        r2 = C.c_double()
+        its = lib().or_solveXX(self.ctx, parity, _p(r), _p(x), m, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+    def solve(self, x, b, m, r2req, maxits=100000):
+        r2 = C.c_double()
+        its = lib().or_solve(self.ctx, _p(x), _p(b), m, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+    def cgm(self, parity, xs, sg, b, m2, r2req, maxits=100000):
+        n = len(xs)
+        arr = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+        sga = (C.c_double * n)(*[float(s) for s in sg])
+        r2 = C.c_double()
+        its = lib().or_cgm_xx(self.ctx, parity, n, arr, sga, _p(b), m2, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+    def solve_multishift(self, xs, b, ms, r2req, maxits=100000):
+        n = len(xs)
+        arr = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+        msa = (C.c_double * n)(*[float(s) for s in ms])
+        r2 = C.c_double()
+        its = lib().or_solve_multishift(self.ctx, n, arr, _p(b), msa, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+    def force_solve(self, psi, phi, m, r2req, maxits=100000):
+        r2 = C.c_double()
+        its = lib().or_force_solve(self.ctx, _p(psi), _p(phi), m, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+    def ferm_force(self, f, psi):
+        lib().or_ferm_force(self.ctx, _p(f), _p(psi))
+
+    def force(self, f, phi, m, r2req, maxits=100000):
+        r2 = C.c_double()
+        its = lib().or_force(self.ctx, _p(f), _p(phi), m, r2req, maxits, C.byref(r2))
+        return its, r2.value
+
+
+def num_threads() -> int:
+    return lib().or_num_threads()

@@ -1,0 +1,120 @@
+"""ctypes binding of ``libqexstag.so`` (the C ABI in ``include/qexstag.h``).
+
+The library is built in-tree by :mod:`qex_b200.build`.  Loading fails loudly
+when it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libqexstag.so"
+
+OK = 0
+NOT_CONVERGED = 1
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_NAN = -3
+ERR_TIMEOUT = -4
+ERR_ALLOC = -5
+ERR_STATE = -6
+
+MEM_HOST = 0
+MEM_DEVICE = 1
+EVEN, ODD, ALL = 0, 1, 2
+SLOPPY_NONE, SLOPPY_SINGLE, SLOPPY_HALF = 0, 1, 2
+
+
+class SolverParamsC(C.Structure):
+    _fields_ = [
+        ("r2req", C.c_double),
+        ("maxits", C.c_int),
+        ("sloppy", C.c_int),
+        ("delta", C.c_double),
+        ("verbosity", C.c_int),
+        ("use_prev_soln", C.c_int),
+        ("reserved", C.c_int * 6),
+    ]
+
+
+class SolverStatsC(C.Structure):
+    _fields_ = [
+        ("calls", C.c_int),
+        ("iterations", C.c_int),
+        ("outer_iterations", C.c_int),
+        ("reliable_updates", C.c_int),
+        ("seconds", C.c_double),
+        ("flops", C.c_double),
+        ("r2", C.c_double),
+        ("kernel_launches", C.c_longlong),
+    ]
+
+
+P = C.c_void_p
+D = C.c_double
+I = C.c_int
+DP = C.POINTER(C.c_double)
+PP = C.POINTER(C.c_void_p)
+
+# name -> (restype, argtypes); every symbol declared in include/qexstag.h
+SIGNATURES = {
+    "qexstag_init": (I, [I]),
+    "qexstag_finalize": (I, []),
+    "qexstag_set_stream": (I, [P]),
+    "qexstag_last_error": (C.c_char_p, []),
+    "qexstag_synchronize": (I, []),
+    "qexstag_layout_create": (I, [C.POINTER(C.c_int), C.POINTER(P)]),
+    "qexstag_layout_destroy": (I, [P]),
+    "qexstag_layout_index": (I, [P, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+    "qexstag_layout_shift_table": (I, [P, I, I, I, P]),
+    "qexstag_links_create": (I, [P, I, P, I, D, C.POINTER(P)]),
+    "qexstag_links_destroy": (I, [P]),
+    "qexstag_links_recon12": (I, [P]),
+    "qexstag_stagD2": (I, [P, I, P, P, D, D, I]),
+    "qexstag_stagD": (I, [P, I, P, P, D, D, D, I]),
+    "qexstag_D": (I, [P, P, P, D, I]),
+    "qexstag_Ddag": (I, [P, P, P, D, I]),
+    "qexstag_stagD2ee": (I, [P, P, P, D, I]),
+    "qexstag_stagD2oo": (I, [P, P, P, D, I]),
+    "qexstag_solveEE": (I, [P, P, P, D, P, P, I]),
+    "qexstag_solveOO": (I, [P, P, P, D, P, P, I]),
+    "qexstag_solve": (I, [P, P, P, D, P, P, I]),
+    "qexstag_solve_multishift": (I, [P, I, PP, P, DP, P, P, I]),
+    "qexstag_cgm_ee": (I, [P, D, I, DP, I, PP, PP, P, P, DP, I]),
+    "qexstag_force": (I, [P, P, P, D, P, P, I]),
+    "qexstag_ferm_force": (I, [P, P, P, I]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the library once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m qex_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class QexStagError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: status {code}: {msg}")
+        self.code = code
+
+
+def check(code: int, where: str, allow_not_converged: bool = True) -> int:
+    if code == OK or (allow_not_converged and code == NOT_CONVERGED):
+        return code
+    msg = load().qexstag_last_error().decode()
+    raise QexStagError(code, where, msg)

@@ -1,0 +1,639 @@
+// api.cu -- the extern "C" entry points declared in include/qexstag.h:
+// argument checking, staging of host fields (QEX V=1 array-of-structs) to the
+// device layout and back, and dispatch to the kernels.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "lib.cuh"
+
+namespace qs {
+
+int build_low_links(qexstag_links_s *g);
+void free_low_links(LowLinks &low);
+int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nrhs,
+           const double2 *const *b, double2 *const *y, const qexstag_solver_params *p,
+           qexstag_solver_stats *st, double *r2_out);
+int solve_multishift(qexstag_links_s *g, int nmass, double2 *const *xs, const double2 *b,
+                     const double *ms, const qexstag_solver_params *p, qexstag_solver_stats *st);
+int apply_D(qexstag_links_s *g, double2 *r, const double2 *x, double m, double sc);
+int stagD_par(qexstag_links_s *g, int par, double2 *r, const double2 *x, double m, double sc,
+              double a);
+
+int Workspace::get(int slot, size_t bytes, void **out) {
+  auto it = bufs.find(slot);
+  if (it != bufs.end() && it->second.first >= bytes) {
+    *out = it->second.second;
+    return QEXSTAG_OK;
+  }
+  if (it != bufs.end()) {
+    cudaStreamSynchronize(stream());
+    cudaFree(it->second.second);
+    bufs.erase(it);
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(QEXSTAG_ERR_ALLOC, std::string("device allocation of ") + std::to_string(bytes) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+  }
+  bufs[slot] = std::make_pair(bytes, p);
+  *out = p;
+  return QEXSTAG_OK;
+}
+
+int Workspace::get_pinned(size_t bytes, void **out) {
+  if (pinned && pinned_bytes >= bytes) {
+    *out = pinned;
+    return QEXSTAG_OK;
+  }
+  if (pinned) {
+    cudaStreamSynchronize(stream());
+    cudaFreeHost(pinned);
+    pinned = nullptr;
+  }
+  cudaError_t e = cudaHostAlloc(&pinned, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    pinned = nullptr;
+    return fail(QEXSTAG_ERR_ALLOC, "pinned host allocation failed");
+  }
+  pinned_bytes = bytes;
+  *out = pinned;
+  return QEXSTAG_OK;
+}
+
+void Workspace::release() {
+  cudaStreamSynchronize(stream());
+  for (auto &kv : bufs) cudaFree(kv.second.second);
+  bufs.clear();
+  if (pinned) cudaFreeHost(pinned);
+  pinned = nullptr;
+  pinned_bytes = 0;
+}
+
+// ---- staging of full-lattice colour vectors ----
+
+// input: returns a device SoA [3][V] view of the field
+static int stage_in(qexstag_links_s *g, int slot, const double *ptr, int mem,
+                    const double2 **dev) {
+  const Geom &geo = g->l->g;
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    *dev = (const double2 *)ptr;
+    return QEXSTAG_OK;
+  }
+  void *soa, *aos;
+  const size_t bytes = sizeof(double2) * 3 * (size_t)geo.V;
+  int rc;
+  if ((rc = g->ws.get(slot, bytes, &soa)) || (rc = g->ws.get(kSlotAos, bytes, &aos))) return rc;
+  QS_CUDA(cudaMemcpyAsync(aos, ptr, bytes, cudaMemcpyHostToDevice, stream()));
+  if ((rc = aos_to_soa((const double *)aos, (double2 *)soa, geo.V, geo.V, 3))) return rc;
+  *dev = (const double2 *)soa;
+  return QEXSTAG_OK;
+}
+
+static int stage_out_buf(qexstag_links_s *g, int slot, double *ptr, int mem, double2 **dev) {
+  const Geom &geo = g->l->g;
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    *dev = (double2 *)ptr;
+    return QEXSTAG_OK;
+  }
+  void *soa;
+  int rc = g->ws.get(slot, sizeof(double2) * 3 * (size_t)geo.V, &soa);
+  if (rc) return rc;
+  *dev = (double2 *)soa;
+  return QEXSTAG_OK;
+}
+
+static int stage_out_finish(qexstag_links_s *g, const double2 *dev, double *ptr, int mem) {
+  if (mem == QEXSTAG_MEM_DEVICE) return QEXSTAG_OK;
+  const Geom &geo = g->l->g;
+  void *aos;
+  const size_t bytes = sizeof(double2) * 3 * (size_t)geo.V;
+  int rc = g->ws.get(kSlotAos, bytes, &aos);
+  if (rc) return rc;
+  if ((rc = soa_to_aos(dev, (double *)aos, geo.V, geo.V, 3))) return rc;
+  QS_CUDA(cudaMemcpyAsync(ptr, aos, bytes, cudaMemcpyDeviceToHost, stream()));
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+static int check_links(const qexstag_links_s *g) {
+  if (!g || !g->l || !g->u64) return fail(QEXSTAG_ERR_ARG, "null or destroyed link handle");
+  int d = -1;
+  cudaGetDevice(&d);
+  if (d != g->l->device) return fail(QEXSTAG_ERR_STATE, "link handle belongs to another device");
+  return runtime_ready();
+}
+
+static int check_mem(int mem) {
+  if (mem != QEXSTAG_MEM_HOST && mem != QEXSTAG_MEM_DEVICE)
+    return fail(QEXSTAG_ERR_ARG, "mem must be QEXSTAG_MEM_HOST or QEXSTAG_MEM_DEVICE");
+  return QEXSTAG_OK;
+}
+
+struct Timer {
+  cudaEvent_t a, b;
+  Timer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, stream());
+  }
+  double seconds() {
+    cudaEventRecord(b, stream());
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3;
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+static void init_stats(qexstag_solver_stats *st) {
+  std::memset(st, 0, sizeof(*st));
+  st->calls = 1;
+  st->kernel_launches = -launch_count();  // completed by finish_stats
+}
+static void finish_stats(qexstag_solver_stats *st) { st->kernel_launches += launch_count(); }
+
+}  // namespace qs
+
+using namespace qs;
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// layout
+// ---------------------------------------------------------------------------
+
+int qexstag_layout_create(const int dims[4], qexstag_layout **out) {
+  if (!dims || !out) return fail(QEXSTAG_ERR_ARG, "layout_create: null argument");
+  long V = 1;
+  for (int d = 0; d < 4; d++) {
+    if (dims[d] < 4 || (dims[d] & 1))
+      return fail(QEXSTAG_ERR_ARG, "layout_create: every dimension must be even and >= 4");
+    V *= dims[d];
+  }
+  if (V * 9 * 8 >= (1L << 31) * 1L && V >= (1L << 28))
+    return fail(QEXSTAG_ERR_ARG, "layout_create: lattice too large");
+  int rc = runtime_ready();
+  if (rc) return rc;
+  qexstag_layout_s *l = new (std::nothrow) qexstag_layout_s;
+  if (!l) return fail(QEXSTAG_ERR_ALLOC, "layout_create: out of host memory");
+  for (int d = 0; d < 4; d++) l->g.L[d] = dims[d];
+  l->g.stride[0] = 1;
+  for (int d = 1; d < 4; d++) l->g.stride[d] = l->g.stride[d - 1] * dims[d - 1];
+  l->g.V = (int)V;
+  l->g.nh = (int)(V / 2);
+  cudaGetDevice(&l->device);
+  *out = l;
+  return QEXSTAG_OK;
+}
+
+int qexstag_layout_destroy(qexstag_layout *l) {
+  delete l;
+  return QEXSTAG_OK;
+}
+
+int qexstag_layout_index(const qexstag_layout *l, const int x[4], int64_t *idx) {
+  if (!l || !x || !idx) return fail(QEXSTAG_ERR_ARG, "layout_index: null argument");
+  const Geom &g = l->g;
+  long lex = 0, p = 0;
+  for (int d = 3; d >= 0; d--) {
+    if (x[d] < 0 || x[d] >= g.L[d]) return fail(QEXSTAG_ERR_ARG, "layout_index: coordinate out of range");
+    lex = lex * g.L[d] + x[d];
+    p += x[d];
+  }
+  *idx = (lex + ((p & 1) ? g.V : 0)) / 2;
+  return QEXSTAG_OK;
+}
+
+}  // extern "C"
+
+namespace qs {
+__global__ void shift_table_kernel(Geom g, int mu, int len, int par, int n, int32_t *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int p = par == 2 ? (i >= g.nh ? 1 : 0) : par;
+    int k = par == 2 ? i - p * g.nh : i;
+    int x[4], lex;
+    site_coords(g, p, k, x, lex);
+    out[i] = (1 - p) * g.nh + nbr_half(g, x, lex, mu, len);
+  }
+}
+}  // namespace qs
+
+extern "C" {
+
+int qexstag_layout_shift_table(const qexstag_layout *l, int mu, int len, int subset,
+                               int32_t *out_host) {
+  if (!l || !out_host) return fail(QEXSTAG_ERR_ARG, "shift_table: null argument");
+  if (mu < 0 || mu > 3 || subset < 0 || subset > 2)
+    return fail(QEXSTAG_ERR_ARG, "shift_table: bad direction or subset");
+  if ((len & 1) == 0 || len > 3 || len < -3)
+    return fail(QEXSTAG_ERR_ARG, "shift_table: len must be +-1 or +-3");
+  int rc = runtime_ready();
+  if (rc) return rc;
+  const Geom &g = l->g;
+  int n = subset == 2 ? g.V : g.nh;
+  int32_t *d = nullptr;
+  QS_CUDA(cudaMalloc(&d, sizeof(int32_t) * n));
+  shift_table_kernel<<<grid_for(n), kBlock, 0, stream()>>>(g, mu, len, subset, n, d);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out_host, d, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream());
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream());
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "shift_table");
+  return QEXSTAG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// links
+// ---------------------------------------------------------------------------
+
+int qexstag_links_create(qexstag_layout *l, int nlinks, const double *links, int mem,
+                         double long_coeff, qexstag_links **out) {
+  if (!l || !links || !out) return fail(QEXSTAG_ERR_ARG, "links_create: null argument");
+  if (nlinks != 4 && nlinks != 8) return fail(QEXSTAG_ERR_ARG, "links_create: nlinks must be 4 or 8");
+  int rc;
+  if ((rc = check_mem(mem)) || (rc = runtime_ready())) return rc;
+  if (long_coeff == 0.0 || !std::isfinite(long_coeff))
+    return fail(QEXSTAG_ERR_ARG, "links_create: long_coeff must be finite and nonzero");
+  qexstag_links_s *g = new (std::nothrow) qexstag_links_s;
+  if (!g) return fail(QEXSTAG_ERR_ALLOC, "links_create: out of host memory");
+  g->l = l;
+  g->nl = nlinks;
+  g->long_coeff = long_coeff;
+  const Geom &geo = l->g;
+  const size_t per = sizeof(double2) * 9 * (size_t)geo.V;
+  cudaError_t e = cudaMalloc(&g->u64, per * nlinks);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete g;
+    return fail(QEXSTAG_ERR_ALLOC, "links_create: device allocation failed");
+  }
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    e = cudaMemcpyAsync(g->u64, links, per * nlinks, cudaMemcpyDeviceToDevice, stream());
+    if (e != cudaSuccess) {
+      cudaFree(g->u64);
+      delete g;
+      return cuda_fail(e, "links_create copy");
+    }
+  } else {
+    void *aos;
+    if ((rc = g->ws.get(kSlotAos, per, &aos))) {
+      cudaFree(g->u64);
+      delete g;
+      return rc;
+    }
+    for (int k = 0; k < nlinks; k++) {
+      e = cudaMemcpyAsync(aos, links + (size_t)k * 18 * geo.V, per, cudaMemcpyHostToDevice, stream());
+      if (e != cudaSuccess) break;
+      if ((rc = aos_to_soa((const double *)aos, g->u64 + (size_t)k * 9 * geo.V, geo.V, geo.V, 9))) break;
+    }
+    if (e != cudaSuccess || rc) {
+      g->ws.release();
+      cudaFree(g->u64);
+      delete g;
+      return e != cudaSuccess ? cuda_fail(e, "links_create upload") : rc;
+    }
+  }
+  if ((rc = build_low_links(g))) {
+    g->ws.release();
+    free_low_links(g->low);
+    cudaFree(g->u64);
+    delete g;
+    return rc;
+  }
+  e = cudaStreamSynchronize(stream());
+  if (e != cudaSuccess) return cuda_fail(e, "links_create");
+  *out = g;
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_destroy(qexstag_links *g) {
+  if (!g) return QEXSTAG_OK;
+  g->ws.release();
+  free_low_links(g->low);
+  cudaFree(g->u64);
+  g->u64 = nullptr;
+  delete g;
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_recon12(const qexstag_links *g) { return (g && g->low.recon12) ? 1 : 0; }
+
+// ---------------------------------------------------------------------------
+// Dslash entry points
+// ---------------------------------------------------------------------------
+
+int qexstag_stagD2(qexstag_links *g, int subset, double *r, const double *x, double a, double b,
+                   int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (!r || !x) return fail(QEXSTAG_ERR_ARG, "stagD2: null field");
+  if (subset != QEXSTAG_EVEN && subset != QEXSTAG_ODD)
+    return fail(QEXSTAG_ERR_ARG, "stagD2: subset must be EVEN or ODD");
+  const Geom &geo = g->l->g;
+  const double2 *dx, *dr_in = nullptr;
+  double2 *dr;
+  if ((rc = stage_in(g, kSlotIn0, x, mem, &dx))) return rc;
+  if ((rc = stage_out_buf(g, kSlotOut0, r, mem, &dr))) return rc;
+  if (mem == QEXSTAG_MEM_HOST) {
+    // r is an input where it is not overwritten: stage all of it
+    if ((rc = stage_in(g, kSlotOut0, r, mem, &dr_in))) return rc;
+  }
+  const int init = (a == 0.0 && b == 0.0) ? 0 : (a == 0.0 ? 1 : 2);
+  rc = dslash64(g, subset, block(dr, geo, subset), block(dx, geo, 1 - subset), block(dx, geo, subset),
+                block((const double2 *)dr, geo, subset), a, b, 1.0, +1, init);
+  if (rc) return rc;
+  return stage_out_finish(g, dr, r, mem);
+}
+
+static int stagD_api(qexstag_links *g, int subset, double *r, const double *x, double m, double sc,
+                     double a, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (!r || !x) return fail(QEXSTAG_ERR_ARG, "stagD: null field");
+  if (subset < 0 || subset > 2) return fail(QEXSTAG_ERR_ARG, "stagD: bad subset");
+  if (sc == 0.0) return fail(QEXSTAG_ERR_ARG, "stagD: sc must be nonzero");
+  const double2 *dx, *dr_in;
+  double2 *dr;
+  if ((rc = stage_in(g, kSlotIn0, x, mem, &dx))) return rc;
+  if ((rc = stage_out_buf(g, kSlotOut0, r, mem, &dr))) return rc;
+  if (mem == QEXSTAG_MEM_HOST && (subset != 2 || a != 0.0)) {
+    if ((rc = stage_in(g, kSlotOut0, r, mem, &dr_in))) return rc;
+  }
+  if (subset == 2) {
+    if ((rc = stagD_par(g, 0, dr, dx, m, sc, a))) return rc;
+    if ((rc = stagD_par(g, 1, dr, dx, m, sc, a))) return rc;
+  } else {
+    if ((rc = stagD_par(g, subset, dr, dx, m, sc, a))) return rc;
+  }
+  return stage_out_finish(g, dr, r, mem);
+}
+
+int qexstag_stagD(qexstag_links *g, int subset, double *r, const double *x, double m, double sc,
+                  double a, int mem) {
+  return stagD_api(g, subset, r, x, m, sc, a, mem);
+}
+int qexstag_D(qexstag_links *g, double *r, const double *x, double m, int mem) {
+  return stagD_api(g, 2, r, x, m, 1.0, 0.0, mem);
+}
+int qexstag_Ddag(qexstag_links *g, double *r, const double *x, double m, int mem) {
+  return stagD_api(g, 2, r, x, m, -1.0, 0.0, mem);
+}
+
+static int schur_api(qexstag_links *g, int par, double *r, const double *x, double m2, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (!r || !x) return fail(QEXSTAG_ERR_ARG, "stagD2ee: null field");
+  const Geom &geo = g->l->g;
+  const double2 *dx, *dr_in;
+  double2 *dr;
+  void *pt;
+  if ((rc = stage_in(g, kSlotIn0, x, mem, &dx))) return rc;
+  if ((rc = stage_out_buf(g, kSlotOut0, r, mem, &dr))) return rc;
+  if (mem == QEXSTAG_MEM_HOST) {
+    if ((rc = stage_in(g, kSlotOut0, r, mem, &dr_in))) return rc;
+  }
+  if ((rc = g->ws.get(kSlotTmpOdd, sizeof(double2) * 3 * (size_t)geo.nh, &pt))) return rc;
+  if ((rc = schur64(g, par, block(dr, geo, par), block(dx, geo, par), VecD{(double2 *)pt, geo.nh}, m2)))
+    return rc;
+  return stage_out_finish(g, dr, r, mem);
+}
+
+int qexstag_stagD2ee(qexstag_links *g, double *r, const double *x, double m2, int mem) {
+  return schur_api(g, 0, r, x, m2, mem);
+}
+int qexstag_stagD2oo(qexstag_links *g, double *r, const double *x, double m2, int mem) {
+  return schur_api(g, 1, r, x, m2, mem);
+}
+
+// ---------------------------------------------------------------------------
+// solvers
+// ---------------------------------------------------------------------------
+
+static int check_params(const qexstag_solver_params *p) {
+  if (!p) return fail(QEXSTAG_ERR_ARG, "null solver params");
+  if (!(p->r2req >= 0.0) || !std::isfinite(p->r2req)) return fail(QEXSTAG_ERR_ARG, "r2req must be >= 0");
+  if (p->sloppy < 0 || p->sloppy > 2) return fail(QEXSTAG_ERR_ARG, "sloppy must be 0, 1 or 2");
+  return QEXSTAG_OK;
+}
+
+static int solveXX_api(qexstag_links *g, int par, double *r, const double *x, double m,
+                       const qexstag_solver_params *p, qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (!r || !x) return fail(QEXSTAG_ERR_ARG, "solveXX: null field");
+  qexstag_solver_stats st;
+  init_stats(&st);
+  const double2 *dx;
+  double2 *dr;
+  Timer tm;
+  if ((rc = stage_in(g, kSlotIn0, x, mem, &dx))) return rc;
+  if ((rc = stage_out_buf(g, kSlotOut0, r, mem, &dr))) return rc;
+  int status = solve_xx(g, par, dr, dx, m, p, &st);
+  if (status < 0) return status;
+  if ((rc = stage_out_finish(g, dr, r, mem))) return rc;
+  st.seconds = tm.seconds();
+  st.flops = (double)(g->nl * 4 * 72 + 60) * g->l->g.nh * st.iterations;
+  finish_stats(&st);
+  if (st_out) *st_out = st;
+  return status;
+}
+
+int qexstag_solveEE(qexstag_links *g, double *r, const double *x, double m,
+                    const qexstag_solver_params *p, qexstag_solver_stats *st, int mem) {
+  return solveXX_api(g, 0, r, x, m, p, st, mem);
+}
+int qexstag_solveOO(qexstag_links *g, double *r, const double *x, double m,
+                    const qexstag_solver_params *p, qexstag_solver_stats *st, int mem) {
+  return solveXX_api(g, 1, r, x, m, p, st, mem);
+}
+
+int qexstag_solve(qexstag_links *g, double *x, const double *b, double m,
+                  const qexstag_solver_params *p, qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (!x || !b) return fail(QEXSTAG_ERR_ARG, "solve: null field");
+  qexstag_solver_stats st;
+  init_stats(&st);
+  const double2 *db;
+  double2 *dx;
+  Timer tm;
+  if ((rc = stage_in(g, kSlotIn0, b, mem, &db))) return rc;
+  if ((rc = stage_out_buf(g, kSlotOut0, x, mem, &dx))) return rc;
+  if (mem == QEXSTAG_MEM_HOST && p->use_prev_soln) {
+    const double2 *tmp;
+    if ((rc = stage_in(g, kSlotOut0, x, mem, &tmp))) return rc;
+  }
+  int status = solve_full(g, dx, db, m, p, &st);
+  if (status < 0) return status;
+  if ((rc = stage_out_finish(g, dx, x, mem))) return rc;
+  st.seconds = tm.seconds();
+  st.flops = (double)(g->nl * 4 * 72 + 60) * g->l->g.nh * st.iterations +
+             (double)(g->nl * 4 * 72 + 24) * g->l->g.nh;
+  finish_stats(&st);
+  if (st_out) *st_out = st;
+  return status;
+}
+
+int qexstag_solve_multishift(qexstag_links *g, int nmass, double *const *xs, const double *b,
+                             const double *ms, const qexstag_solver_params *p,
+                             qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (nmass < 1 || nmass > 64 || !xs || !b || !ms)
+    return fail(QEXSTAG_ERR_ARG, "solve_multishift: need 1..64 masses and non-null fields");
+  for (int k = 0; k < nmass; k++)
+    if (!xs[k]) return fail(QEXSTAG_ERR_ARG, "solve_multishift: null output field");
+  const Geom &geo = g->l->g;
+  qexstag_solver_stats st;
+  init_stats(&st);
+  Timer tm;
+  const double2 *db;
+  if ((rc = stage_in(g, kSlotIn0, b, mem, &db))) return rc;
+  double2 *dxs[64];
+  for (int k = 0; k < nmass; k++) {
+    if (mem == QEXSTAG_MEM_DEVICE) {
+      dxs[k] = (double2 *)xs[k];
+    } else {
+      void *q;
+      if ((rc = g->ws.get(kSlotMs0 + 100 + k, sizeof(double2) * 3 * (size_t)geo.V, &q))) return rc;
+      dxs[k] = (double2 *)q;
+    }
+  }
+  int status = solve_multishift(g, nmass, dxs, db, ms, p, &st);
+  if (status < 0) return status;
+  for (int k = 0; k < nmass; k++)
+    if ((rc = stage_out_finish(g, dxs[k], xs[k], mem))) return rc;
+  st.seconds = tm.seconds();
+  finish_stats(&st);
+  if (st_out) *st_out = st;
+  return status;
+}
+
+int qexstag_cgm_ee(qexstag_links *g, double m, int nshift, const double *sigma, int nrhs,
+                   const double *const *b, double *const *y, const qexstag_solver_params *p,
+                   qexstag_solver_stats *st_out, double *r2_out, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (nshift < 1 || nshift > 32 || nrhs < 1 || nrhs > 16 || !sigma || !b || !y)
+    return fail(QEXSTAG_ERR_ARG, "cgm_ee: need 1..32 shifts, 1..16 right-hand sides");
+  for (int k = 0; k < nshift; k++)
+    if (!(sigma[k] >= 0.0)) return fail(QEXSTAG_ERR_ARG, "cgm_ee: shifts must be >= 0");
+  const Geom &geo = g->l->g;
+  qexstag_solver_stats st;
+  init_stats(&st);
+  Timer tm;
+  const size_t fb = sizeof(double2) * 3 * (size_t)geo.V;
+  const double2 *db[16];
+  double2 *dy[16 * 32];
+  for (int j = 0; j < nrhs; j++) {
+    if (!b[j]) return fail(QEXSTAG_ERR_ARG, "cgm_ee: null right-hand side");
+    if ((rc = stage_in(g, kSlotMs0 + j, b[j], mem, &db[j]))) return rc;
+  }
+  for (int i = 0; i < nrhs * nshift; i++) {
+    if (!y[i]) return fail(QEXSTAG_ERR_ARG, "cgm_ee: null solution field");
+    if (mem == QEXSTAG_MEM_DEVICE) {
+      dy[i] = (double2 *)y[i];
+    } else {
+      void *q;
+      if ((rc = g->ws.get(kSlotLast + i, fb, &q))) return rc;
+      dy[i] = (double2 *)q;
+    }
+  }
+  int status = cgm_ee(g, m, nshift, sigma, nrhs, db, dy, p, &st, r2_out);
+  if (status < 0) return status;
+  for (int i = 0; i < nrhs * nshift; i++)
+    if ((rc = stage_out_finish(g, dy[i], y[i], mem))) return rc;
+  st.seconds = tm.seconds();
+  finish_stats(&st);
+  if (st_out) *st_out = st;
+  return status;
+}
+
+// ---------------------------------------------------------------------------
+// force
+// ---------------------------------------------------------------------------
+
+static int force_out(qexstag_links *g, double2 *df, double *f, int mem) {
+  if (mem == QEXSTAG_MEM_DEVICE) return QEXSTAG_OK;
+  const Geom &geo = g->l->g;
+  const size_t per = sizeof(double2) * 9 * (size_t)geo.V;
+  void *aos;
+  int rc = g->ws.get(kSlotAos, per, &aos);
+  if (rc) return rc;
+  for (int k = 0; k < g->nl; k++) {
+    if ((rc = soa_to_aos(df + (size_t)k * 9 * geo.V, (double *)aos, geo.V, geo.V, 9))) return rc;
+    QS_CUDA(cudaMemcpyAsync(f + (size_t)k * 18 * geo.V, aos, per, cudaMemcpyDeviceToHost, stream()));
+  }
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+static int force_buf(qexstag_links *g, double *f, int mem, double2 **df) {
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    *df = (double2 *)f;
+    return QEXSTAG_OK;
+  }
+  void *q;
+  int rc = g->ws.get(kSlotLast + 600, sizeof(double2) * 9 * (size_t)g->l->g.V * g->nl, &q);
+  *df = (double2 *)q;
+  return rc;
+}
+
+int qexstag_ferm_force(qexstag_links *g, double *f, const double *psi, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (!f || !psi) return fail(QEXSTAG_ERR_ARG, "ferm_force: null field");
+  const double2 *dpsi;
+  double2 *df;
+  if ((rc = stage_in(g, kSlotIn0, psi, mem, &dpsi))) return rc;
+  if ((rc = force_buf(g, f, mem, &df))) return rc;
+  if ((rc = ferm_force64(g, df, dpsi))) return rc;
+  return force_out(g, df, f, mem);
+}
+
+int qexstag_force(qexstag_links *g, double *f, const double *phi, double m,
+                  const qexstag_solver_params *p, qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (!f || !phi) return fail(QEXSTAG_ERR_ARG, "force: null field");
+  const Geom &geo = g->l->g;
+  qexstag_solver_stats st;
+  init_stats(&st);
+  Timer tm;
+  const double2 *dphi;
+  double2 *df;
+  void *pvar, *ppsi;
+  const size_t fb = sizeof(double2) * 3 * (size_t)geo.V;
+  if ((rc = stage_in(g, kSlotIn0, phi, mem, &dphi))) return rc;
+  if ((rc = force_buf(g, f, mem, &df))) return rc;
+  if ((rc = g->ws.get(kSlotFull1, fb, &pvar)) || (rc = g->ws.get(kSlotIn1, fb, &ppsi))) return rc;
+  double2 *varphi = (double2 *)pvar, *psi = (double2 *)ppsi;
+  // stagForceSolve (hmcAction.nim:669-721)
+  int status = solve_xx(g, 0, varphi, dphi, m, p, &st);
+  if (status < 0) return status;
+  if ((rc = vscale(block(varphi, geo, 0), 4.0, geo.nh))) return rc;
+  // psi_o = (2D)_oe varphi_e (stagD2 with a = b = 0); psi_e = varphi_e
+  if ((rc = dslash64(g, 1, block(psi, geo, 1), block((const double2 *)varphi, geo, 0),
+                     CVecD{nullptr, 0}, CVecD{nullptr, 0}, 0.0, 0.0, 1.0, +1, 0)))
+    return rc;
+  if ((rc = vcopy(block(psi, geo, 0), block((const double2 *)varphi, geo, 0), geo.nh))) return rc;
+  if ((rc = ferm_force64(g, df, psi))) return rc;
+  if ((rc = force_out(g, df, f, mem))) return rc;
+  st.seconds = tm.seconds();
+  st.flops = (double)(g->nl * 4 * 72 + 60) * geo.nh * st.iterations;
+  finish_stats(&st);
+  if (st_out) *st_out = st;
+  return status;
+}
+
+}  // extern "C"

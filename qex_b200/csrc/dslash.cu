@@ -1,0 +1,211 @@
+// dslash.cu -- FP64 even-odd staggered Dslash (naive and fat+Naik) and the
+// Schur operator built from two half sweeps.
+//
+// One thread per output site.  For each hop k the thread gathers the input
+// colour vector at s+d_k and s-d_k (other parity; neighbours of consecutive
+// sites are nearly consecutive, so these gathers coalesce and the other-parity
+// vector is served from L2 after its first read), streams the 9 complex
+// elements of U_k(s) and of U_k(s-d_k) as 16-byte words, and accumulates
+// U_k(s) x(s+d_k) - U_k(s-d_k)^dagger x(s-d_k) in registers (QEX stagD2,
+// src/physics/stagD.nim:383-448: per k forward then backward, after the
+// a*r + b*x init).  Neighbour indices come from the site coordinates
+// (src/layout/qlayout.nim:108-136) rather than from tables, which saves
+// 4 bytes per hop per site of HBM traffic.
+//
+// Compulsory HBM bytes per output site: 8 (naive) or 16 (fat+Naik) links of
+// 144 B, plus 48 B in, 48 B out, plus 48 B per same-site init operand.
+#include "lib.cuh"
+
+namespace qs {
+
+struct DslashArgs64 {
+  Geom g;
+  int po;
+  const double2 *__restrict__ u;
+  const double2 *__restrict__ xin;
+  int istride;
+  const double2 *xs;  // may alias out (same site, read before the write)
+  int sstride;
+  const double2 *rin;  // may alias out
+  int rstride;
+  double2 *out;
+  int ostride;
+  double a, b, c;
+  const int *done;
+  CgState *state;
+  double *partials;
+  unsigned *ticket;
+  double *dot_out;
+};
+
+template <int NL, int HOP, int INIT, int RED>
+__global__ void __launch_bounds__(kBlock) dslash64_kernel(const DslashArgs64 A) {
+  if (A.done != nullptr && *A.done) return;
+  const Geom &g = A.g;
+  const int nh = g.nh;
+  const size_t V = (size_t)g.V;
+  const size_t in_base = (size_t)(1 - A.po) * nh;
+  const size_t out_base = (size_t)A.po * nh;
+  double dot = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+    int x[4], lex;
+    site_coords(g, A.po, k, x, lex);
+    double2 acc[3];
+    double2 xsv[3];
+    if (INIT == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[c] = make_double2(0.0, 0.0);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        xsv[c] = __ldcg(A.xs + (size_t)c * A.sstride + k);
+        acc[c] = make_double2(A.b * xsv[c].x, A.b * xsv[c].y);
+      }
+      if (INIT == 2) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          double2 rv = __ldcg(A.rin + (size_t)c * A.rstride + k);
+          acc[c].x = fma(A.a, rv.x, acc[c].x);
+          acc[c].y = fma(A.a, rv.y, acc[c].y);
+        }
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < NL; l++) {
+      const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
+      const int jf = nbr_half(g, x, lex, mu, len);
+      const int jb = nbr_half(g, x, lex, mu, -len);
+      const double2 *ul = A.u + (size_t)l * 9 * V;
+      double2 v[3], w[3], uf[9], ub[9];
+#pragma unroll
+      for (int c = 0; c < 3; c++) v[c] = ldg(A.xin + (size_t)c * A.istride + jf);
+#pragma unroll
+      for (int e = 0; e < 9; e++) uf[e] = ldlink(ul + (size_t)e * V + out_base + k);
+#pragma unroll
+      for (int c = 0; c < 3; c++) w[c] = ldg(A.xin + (size_t)c * A.istride + jb);
+#pragma unroll
+      for (int e = 0; e < 9; e++) ub[e] = ldlink(ul + (size_t)e * V + in_base + jb);
+      double2 t[3], q[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        t[i] = make_double2(0.0, 0.0);
+        q[i] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          t[i] = cmadd(t[i], uf[3 * i + j], v[j]);
+          q[i] = cjmadd(q[i], ub[3 * j + i], w[j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        if (HOP > 0) {
+          acc[i].x += t[i].x;
+          acc[i].y += t[i].y;
+          acc[i].x -= q[i].x;
+          acc[i].y -= q[i].y;
+        } else {
+          acc[i].x -= t[i].x;
+          acc[i].y -= t[i].y;
+          acc[i].x += q[i].x;
+          acc[i].y += q[i].y;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double2 o = make_double2(A.c * acc[c].x, A.c * acc[c].y);
+      A.out[(size_t)c * A.ostride + k] = o;
+      if (RED != kRedNone) {
+        // Re <xs, out>, xs is the same-site operand (p in CG's A p)
+        dot = fma(xsv[c].x, o.x, dot);
+        dot = fma(xsv[c].y, o.y, dot);
+      }
+    }
+  }
+  if (RED != kRedNone) {
+    double v[1] = {dot}, s[1];
+    if (grid_reduce<1>(v, A.partials, A.ticket, s) && threadIdx.x == 0) {
+      if (RED == kRedCgPAp) {
+        // cg.nim:213-215: qLAp = <q, LAp>, alpha = rz/qLAp; itn counted at Ap
+        CgState *st = A.state;
+        st->pAp = s[0];
+        st->alpha = st->rz / s[0];
+        st->itn += 1;
+      } else {
+        *A.dot_out = s[0];
+      }
+    }
+  }
+  (void)out_base;
+}
+
+template <int NL, int HOP, int INIT, int RED>
+static void launch64(const DslashArgs64 &A, int grid) {
+  dslash64_kernel<NL, HOP, INIT, RED><<<grid, kBlock, 0, stream()>>>(A);
+  note_launch();
+}
+
+template <int NL>
+static int dispatch64(const DslashArgs64 &A, int hop, int init, int red, int grid) {
+#define QS_D64(H, I, R)                                            \
+  if (hop == H && init == I && red == R) {                         \
+    launch64<NL, H, I, R>(A, grid);                                \
+    return QEXSTAG_OK;                                             \
+  }
+  QS_D64(1, 0, kRedNone)
+  QS_D64(1, 1, kRedNone)
+  QS_D64(1, 2, kRedNone)
+  QS_D64(-1, 0, kRedNone)
+  QS_D64(-1, 1, kRedNone)
+  QS_D64(-1, 2, kRedNone)
+  QS_D64(-1, 1, kRedCgPAp)
+  QS_D64(-1, 1, kRedDot)
+#undef QS_D64
+  return fail(QEXSTAG_ERR_ARG, "dslash64: unsupported variant");
+}
+
+int dslash64(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, CVecD rin,
+             double a, double b, double c, int hop, int init, int red, void *state,
+             const int *done, double *dot_out) {
+  const Geom &g = gl->l->g;
+  DslashArgs64 A;
+  A.g = g;
+  A.po = po;
+  A.u = gl->u64;
+  A.xin = xin.p;
+  A.istride = xin.stride;
+  A.xs = xs.p;
+  A.sstride = xs.stride;
+  A.rin = rin.p;
+  A.rstride = rin.stride;
+  A.out = out.p;
+  A.ostride = out.stride;
+  A.a = a;
+  A.b = b;
+  A.c = c;
+  A.done = done;
+  A.state = (CgState *)state;
+  A.partials = red_partials();
+  A.ticket = red_tickets();
+  A.dot_out = dot_out;
+  int grid = grid_for(g.nh, kBlock, 6);
+  if (red != kRedNone && grid > kMaxRedBlocks) grid = kMaxRedBlocks;
+  int rc = (gl->nl == 8) ? dispatch64<8>(A, hop, init, red, grid)
+                         : dispatch64<4>(A, hop, init, red, grid);
+  if (rc) return rc;
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
+// stagD2xx (stagD.nim:485-512): t_q = (2D)_{q,par} x (stagDP, rir := 0), then
+// r = 4 m2 x - (2D)_{par,q} t (stagDM with rir := 4 m2 x).
+int schur64(const qexstag_links_s *gl, int par, VecD r, CVecD x, VecD t, double m2, int red,
+            void *state, const int *done, double *dot_out) {
+  int rc = dslash64(gl, 1 - par, t, x, CVecD{nullptr, 0}, CVecD{nullptr, 0}, 0.0, 0.0, 1.0, +1,
+                    0, kRedNone, nullptr, done);
+  if (rc) return rc;
+  return dslash64(gl, par, r, cv(t), x, CVecD{nullptr, 0}, 0.0, 4.0 * m2, 1.0, -1, 1, red, state,
+                  done, dot_out);
+}
+
+}  // namespace qs

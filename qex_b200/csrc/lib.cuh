@@ -1,0 +1,121 @@
+// lib.cuh -- host-side declarations shared between the library's
+// translation units: the link handle, its device workspace and the kernel
+// launchers.
+#pragma once
+#include <map>
+#include <vector>
+
+#include "internal.cuh"
+#include "mixed.cuh"
+
+namespace qs {
+
+int runtime_ready();
+
+// Device workspace owned by a link handle: buffers identified by a slot
+// number, grown on demand, freed with the handle.
+struct Workspace {
+  std::map<int, std::pair<size_t, void *>> bufs;
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
+  int get(int slot, size_t bytes, void **out);
+  int get_pinned(size_t bytes, void **out);
+  void release();
+};
+
+// workspace slots
+enum Slot {
+  kSlotIn0 = 0,   // staged host input fields (SoA)
+  kSlotIn1,
+  kSlotOut0,      // staged outputs (SoA)
+  kSlotOut1,
+  kSlotAos,       // AoS staging for host transfers
+  kSlotTmpOdd,    // stagD2xx temporary (other parity block)
+  kSlotCgR, kSlotCgP, kSlotCgAp, kSlotCgT, kSlotCgX,
+  kSlotCgState,
+  kSlotDcRho, kSlotDcY, kSlotDcB,  // defect correction
+  kSlotFull0, kSlotFull1, kSlotFull2,
+  kSlotMx0 = 40,  // mixed-precision vectors and multishift (up to 80 slots)
+  kSlotMs0 = 120,
+  kSlotLast = 400
+};
+
+}  // namespace qs
+
+struct qexstag_links_s {
+  qexstag_layout_s *l = nullptr;
+  int nl = 0;
+  double long_coeff = 1.0;
+  double2 *u64 = nullptr;  // [nl][9][V]
+  qs::LowLinks low;        // FP32 / FP16 copies (mixed.cuh)
+  qs::Workspace ws;
+};
+
+namespace qs {
+
+// a colour-vector view: SoA double2 [3][stride], sites indexed from 0
+struct VecD {
+  double2 *p;
+  int stride;
+};
+struct CVecD {
+  const double2 *p;
+  int stride;
+};
+inline CVecD cv(VecD v) { return CVecD{v.p, v.stride}; }
+// parity block of a full-lattice field
+inline VecD block(double2 *full, const Geom &g, int par) { return VecD{full + (size_t)par * g.nh, g.V}; }
+inline CVecD block(const double2 *full, const Geom &g, int par) {
+  return CVecD{full + (size_t)par * g.nh, g.V};
+}
+
+// ---- dslash.cu ----
+// out = c*(a*rin + b*xs + hop*sum_k [...]) on the output parity po, with
+// input field xin on the other parity and xs, rin on parity po.
+// init: 0 -> zero, 1 -> b*xs, 2 -> a*rin + b*xs.
+enum RedKind { kRedNone = 0, kRedCgPAp = 1, kRedDot = 2 };
+int dslash64(const qexstag_links_s *g, int po, VecD out, CVecD xin, CVecD xs, CVecD rin,
+             double a, double b, double c, int hop, int init, int red = kRedNone,
+             void *state = nullptr, const int *done = nullptr, double *dot_out = nullptr);
+// Schur operator on parity par: r = 4 m2 x - (2D)_{par,q} (2D)_{q,par} x,
+// with t (q block) the temporary; red kRedCgPAp/kRedDot accumulate Re<x, r>.
+int schur64(const qexstag_links_s *g, int par, VecD r, CVecD x, VecD t, double m2,
+            int red = kRedNone, void *state = nullptr, const int *done = nullptr,
+            double *dot_out = nullptr);
+
+// ---- blas.cu ----
+int aos_to_soa(const double *aos, double2 *soa, int n, int stride, int ncomp);
+int soa_to_aos(const double2 *soa, double *aos, int n, int stride, int ncomp);
+int vcopy(VecD y, CVecD x, int n);
+int vzero(VecD y, int n);
+int vscale(VecD y, double s, int n);
+int vaxpy(VecD y, double a, CVecD x, int n);         // y += a x
+int vxpay(VecD y, CVecD x, double a, int n);         // y = x + a y
+int vaxpby(VecD y, double a, CVecD x, double b, int n);  // y = a x + b y
+int vsub(VecD y, CVecD a, CVecD b, int n);           // y = a - b
+// reductions to a device double (result) and, when host != nullptr, to host
+int vnorm2(CVecD x, int n, double *host);
+int vredot(CVecD x, CVecD y, int n, double *host);
+// |a - b|^2 (no write)
+int vdiffnorm2(CVecD a, CVecD b, int n, double *host);
+
+// ---- solvers (cg.cu) ----
+struct CgOut {
+  int iterations;
+  double r2;  // recursive |r|^2/|b|^2 at exit
+  int nan;
+};
+// FP64 CG (cg.nim, cpNone) on parity par for stagD2xx(m2) x = b, x zeroed.
+int cg64(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, int maxits,
+         CgOut *out);
+// solveXX (stagSolve.nim:330-421): defect correction with inner solver of
+// precision sloppy; r, x full-lattice device fields.
+int solve_xx(qexstag_links_s *g, int par, double2 *r, const double2 *x, double m,
+             const qexstag_solver_params *p, qexstag_solver_stats *st);
+int solve_full(qexstag_links_s *g, double2 *x, const double2 *b, double m,
+               const qexstag_solver_params *p, qexstag_solver_stats *st);
+
+// ---- force.cu ----
+int ferm_force64(qexstag_links_s *g, double2 *f, const double2 *psi);
+
+}  // namespace qs

@@ -1,0 +1,126 @@
+"""GPU parity of the layout tables and the FP64 Dslash family against the
+oracle, through the C ABI (host and device paths).  Tolerance 1e-13
+relative (max-norm), bit-exact for index tables."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qex_b200 import _lib as L
+from qex_b200 import fields as F
+from qex_b200 import stag as S
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+SHAPES = [(8, 8, 8, 8), (4, 6, 8, 4), (6, 4, 4, 10)]
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def links_for(dims, naik, seed=3):
+    return F.fat_naik_links(dims, seed) if naik else F.naive_links(dims, 0.3, seed)
+
+
+@pytest.mark.parametrize("dims", SHAPES)
+def test_shift_tables_bit_exact(cuda, dims):
+    lay = S.Layout(dims)
+    V = F.volume(dims)
+    for mu in range(4):
+        for ln in (1, -1, 3, -3):
+            for sub in (0, 1, 2):
+                got = lay.shift_table(mu, ln, sub)
+                exp = O.shift_table(dims, mu, ln, sub)
+                assert np.array_equal(got, exp), (mu, ln, sub)
+    c = F.coords(dims)
+    for i in range(0, V, max(1, V // 50)):
+        assert lay.index(c[i]) == i
+
+
+@pytest.mark.parametrize("naik", [False, True])
+@pytest.mark.parametrize("dims", SHAPES)
+def test_dslash_family_host_path(cuda, dims, naik):
+    V = F.volume(dims)
+    g = links_for(dims, naik)
+    o = O.Oracle(dims, g)
+    lay = S.Layout(dims)
+    s = S.Staggered(lay, g)
+    x = F.gaussian_vector(V, 5)
+    r0 = F.gaussian_vector(V, 6)
+    for sub in (0, 1):
+        for a, b in [(0.0, 0.0), (0.0, 0.7), (0.3, -1.2)]:
+            rg, ro = r0.copy(), r0.copy()
+            s.stagD2(sub, rg, x, a, b)
+            o.stagD2(sub, ro, x, a, b)
+            assert rel(rg, ro) < TOL, (sub, a, b)
+        for m, sc, a in [(0.1, 1.0, 0.0), (0.2, -1.0, 0.0), (0.05, 1.0, 0.4)]:
+            rg, ro = r0.copy(), r0.copy()
+            s.stagD(sub, rg, x, m, sc, a)
+            o.stagD(sub, ro, x, m, sc, a)
+            assert rel(rg, ro) < TOL
+    for fn in ("D", "Ddag"):
+        rg, ro = o.vec(), o.vec()
+        getattr(s, fn)(rg, x, 0.1)
+        getattr(o, fn)(ro, x, 0.1)
+        assert rel(rg, ro) < TOL
+    for fn in ("stagD2ee", "stagD2oo"):
+        rg, ro = r0.copy(), r0.copy()
+        getattr(s, fn)(rg, x, 0.01)
+        getattr(o, fn)(ro, x, 0.01)
+        par = 0 if fn == "stagD2ee" else 1
+        sl = slice(0, V // 2) if par == 0 else slice(V // 2, V)
+        assert rel(rg[sl], ro[sl]) < TOL
+        other = slice(V // 2, V) if par == 0 else slice(0, V // 2)
+        assert np.array_equal(rg[other], r0[other])
+
+
+@pytest.mark.parametrize("naik", [False, True])
+def test_dslash_device_path_matches_host(cuda, naik):
+    torch = cuda
+    dims = (8, 8, 8, 8)
+    V = F.volume(dims)
+    g = links_for(dims, naik)
+    lay = S.Layout(dims)
+    sh = S.Staggered(lay, g)
+    sd = S.Staggered(lay, S.to_device_links(g))
+    x = F.gaussian_vector(V, 8)
+    rh = np.zeros((V, 3), complex)
+    sh.D(rh, x, 0.3)
+    xd = S.to_device_vector(x)
+    rd = torch.zeros((3, V), dtype=torch.complex128, device="cuda")
+    sd.D(rd, xd, 0.3)
+    assert np.array_equal(S.to_host_vector(rd), rh)
+    sd.stagD2ee(rd, xd, 0.09)
+    o = O.Oracle(dims, g)
+    ro = o.vec()
+    o.stagD2ee(ro, x, 0.09)
+    assert rel(S.to_host_vector(rd)[: V // 2], ro[: V // 2]) < TOL
+
+
+def test_dslash_deterministic(cuda):
+    dims = (8, 8, 8, 8)
+    V = F.volume(dims)
+    g = links_for(dims, True)
+    s = S.Staggered(S.Layout(dims), g)
+    x = F.gaussian_vector(V, 9)
+    a, b = np.zeros((V, 3), complex), np.zeros((V, 3), complex)
+    s.D(a, x, 0.1)
+    s.D(b, x, 0.1)
+    assert np.array_equal(a, b)
+
+
+def test_argument_errors(cuda):
+    dims = (4, 4, 4, 4)
+    lay = S.Layout(dims)
+    with pytest.raises(L.QexStagError) as e:
+        S.Layout((4, 4, 5, 4))
+    assert e.value.code == L.ERR_ARG
+    g = links_for(dims, False)
+    s = S.Staggered(lay, g)
+    V = lay.V
+    x = np.zeros((V, 3), complex)
+    with pytest.raises(L.QexStagError) as e:
+        s.stagD2(2, x.copy(), x, 0.0, 1.0)
+    assert e.value.code == L.ERR_ARG
+    lib = L.load()
+    assert lib.qexstag_links_create(lay.handle, 5, None, 0, 1.0, None) == L.ERR_ARG
