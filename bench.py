@@ -215,7 +215,8 @@ def run_ours(args, dims):
     bd = S.to_device_vector(b)
     yd = torch.zeros((3, V), dtype=torch.complex128, device="cuda")
 
-    configs = [("fp64", {"sloppySolve": 0})]
+    configs = [("fp64", {"sloppySolve": 0}), ("fp32+fp64", {"sloppySolve": 1}),
+               ("fp16+fp64", {"sloppySolve": 2})]
     results = {}
     for name, kw in configs:
         # warm-up

@@ -206,6 +206,16 @@ int qexstag_force(qexstag_links *g, double *f, const double *phi, double m,
 /* fermForce alone for a given psi (full lattice). */
 int qexstag_ferm_force(qexstag_links *g, double *f, const double *psi, int mem);
 
+/* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
+   the same way, host timers around repeated calls) ---- */
+
+/* Time the even-parity Schur operator (two Dslash half sweeps) in precision
+   prec (0 FP64, 1 FP32, 2 FP16 with the handle's reduced-precision links) on
+   internal device vectors: seconds per call, averaged over nrep calls after
+   two warm-up calls, from CUDA events on the library's stream. */
+int qexstag_bench_schur(qexstag_links *g, int prec, int nrep, double m2,
+                        double *seconds_per_call);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,7 @@ SIGNATURES = {
     "qexstag_cgm_ee": (I, [P, D, I, DP, I, PP, PP, P, P, DP, I]),
     "qexstag_force": (I, [P, P, P, D, P, P, I]),
     "qexstag_ferm_force": (I, [P, P, P, I]),
+    "qexstag_bench_schur": (I, [P, I, I, D, DP]),
 }
 
 _lib = None

@@ -214,6 +214,7 @@ int solve_xx(qexstag_links_s *g, int par, double2 *r, const double2 *x, double m
   if ((rc = vcopy(rho, xpar, nh))) return rc;
   double b2 = 0;
   if ((rc = vnorm2(cv(rho), nh, &b2))) return rc;
+  if (!std::isfinite(b2)) return fail(QEXSTAG_ERR_NAN, "solveXX: source is not finite");
   double r2 = b2, r2stop = p->r2req * b2, r2prev = INFINITY;
   const int maxits = p->maxits > 0 ? p->maxits : 50000;
   while (r2 > r2stop && r2 < r2prev) {
@@ -315,6 +316,7 @@ int solve_full(qexstag_links_s *g, double2 *x, const double2 *b, double m,
   VecD xf{x, V}, rf{r, V};
   double b2 = 0;
   if ((rc = vnorm2(CVecD{b, V}, V, &b2))) return rc;
+  if (!std::isfinite(b2)) return fail(QEXSTAG_ERR_NAN, "solve: source is not finite");
   double r2stop = p->r2req * b2;
   if (p->use_prev_soln) {
     if ((rc = apply_D(g, r, x, m, 1.0))) return rc;

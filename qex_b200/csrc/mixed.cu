@@ -1,14 +1,219 @@
-// mixed.cu -- reduced-precision link copies, the sloppy (FP32 / FP16)
-// reliable-update CG and the multi-shift solvers.
+// mixed.cu -- reduced-precision link copies, the FP32 / FP16 Dslash and the
+// reliable-update mixed-precision CG.
+//
+// Mixed-precision CG.  QEX's own sloppy solve (stagSolve.nim:101-117) is an
+// FP32 CG inside FP64 defect correction, floored at FP32 epsilon.  Here the
+// inner solver is a reliable-update CG (Sleijpen and van der Vorst 1996, the
+// scheme QUDA uses): iterate in the sloppy precision, keep the solution
+// increment in FP32, and whenever the iterated residual has dropped by delta
+// since the last update (or the solve appears converged) fold the increment
+// into the FP64 solution, recompute the true FP64 residual b - A x with the
+// FP64 operator, restart the sloppy residual from it and re-orthogonalise
+// the search direction.  All dot products and norms accumulate in FP64.
+// The FP64 defect-correction loop of solveXX wraps this solver unchanged.
+//
+// Sloppy Dslash traffic per output site, fat+Naik with 12-real long links:
+//   FP32: 4*(72+72)+4*(48+48) links + 24 in + 24 out = 1008 B
+//   FP16: 4*(36+36)+4*(24+24) links + 16 in + 16 out = 512 B
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
 #include "lib.cuh"
+#include "lowprec.cuh"
 
 namespace qs {
 
+// ---------------------------------------------------------------------------
+// building the reduced-precision copies
+// ---------------------------------------------------------------------------
+
+__global__ void absmax_kernel(const double2 *__restrict__ u, size_t n, unsigned *out) {
+  float m = 0.f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 v = u[i];
+    m = fmaxf(m, (float)fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // m >= 0: uint order = float order
+}
+
+// max over long links of |row2 - (s/c) conj(row0 x row1)| / |c|
+__global__ void recon_check_kernel(Geom g, const double2 *__restrict__ u64, double c, unsigned *out) {
+  const size_t V = g.V;
+  float m = 0.f;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * g.V; t += gridDim.x * blockDim.x) {
+    const int mu = t / g.V, site = t - mu * g.V;
+    const int par = site >= g.nh ? 1 : 0;
+    int x[4], lex;
+    site_coords(g, par, site - par * g.nh, x, lex);
+    double s = long_sign_fwd(g, x, mu);
+    const double2 *ul = u64 + (size_t)(2 * mu + 1) * 9 * V + site;
+    double2 e[9];
+    for (int j = 0; j < 9; j++) e[j] = ul[(size_t)j * V];
+    double2 cr[3];
+    for (int i = 0; i < 3; i++) {
+      int j = (i + 1) % 3, k = (i + 2) % 3;
+      double2 a = e[j], b = e[3 + k], a2 = e[k], b2 = e[3 + j];
+      cr[i] = make_double2(a.x * b.x - a.y * b.y - (a2.x * b2.x - a2.y * b2.y),
+                           a.x * b.y + a.y * b.x - (a2.x * b2.y + a2.y * b2.x));
+    }
+    double k = s / c, d = 0;
+    for (int i = 0; i < 3; i++) {
+      d = fmax(d, fabs(e[6 + i].x - k * cr[i].x));
+      d = fmax(d, fabs(e[6 + i].y + k * cr[i].y));
+    }
+    m = fmaxf(m, (float)(d / fabs(c)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// FP32/FP16 copy of link k (all sites) into list slot f
+__global__ void to_low18_kernel(const double2 *__restrict__ uk, size_t V, float4 *c32, float2 *t32,
+                                uint4 *c16, unsigned *t16, int f, float inv16) {
+  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < V; s += (size_t)gridDim.x * blockDim.x) {
+    double2 e[9];
+    for (int j = 0; j < 9; j++) e[j] = uk[(size_t)j * V + s];
+    for (int j = 0; j < 4; j++)
+      c32[((size_t)f * 4 + j) * V + s] =
+          make_float4((float)e[2 * j].x, (float)e[2 * j].y, (float)e[2 * j + 1].x, (float)e[2 * j + 1].y);
+    t32[(size_t)f * V + s] = make_float2((float)e[8].x, (float)e[8].y);
+    for (int j = 0; j < 2; j++) {
+      uint4 q;
+      q.x = f2h((float)(e[4 * j].x * inv16), (float)(e[4 * j].y * inv16));
+      q.y = f2h((float)(e[4 * j + 1].x * inv16), (float)(e[4 * j + 1].y * inv16));
+      q.z = f2h((float)(e[4 * j + 2].x * inv16), (float)(e[4 * j + 2].y * inv16));
+      q.w = f2h((float)(e[4 * j + 3].x * inv16), (float)(e[4 * j + 3].y * inv16));
+      c16[((size_t)f * 2 + j) * V + s] = q;
+    }
+    t16[(size_t)f * V + s] = f2h((float)(e[8].x * inv16), (float)(e[8].y * inv16));
+  }
+}
+
+__global__ void to_low12_kernel(const double2 *__restrict__ uk, size_t V, float4 *c32, uint4 *c16,
+                                uint2 *t16, int f, float inv16) {
+  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < V; s += (size_t)gridDim.x * blockDim.x) {
+    double2 e[6];
+    for (int j = 0; j < 6; j++) e[j] = uk[(size_t)j * V + s];
+    for (int j = 0; j < 3; j++)
+      c32[((size_t)f * 3 + j) * V + s] =
+          make_float4((float)e[2 * j].x, (float)e[2 * j].y, (float)e[2 * j + 1].x, (float)e[2 * j + 1].y);
+    uint4 q;
+    q.x = f2h((float)(e[0].x * inv16), (float)(e[0].y * inv16));
+    q.y = f2h((float)(e[1].x * inv16), (float)(e[1].y * inv16));
+    q.z = f2h((float)(e[2].x * inv16), (float)(e[2].y * inv16));
+    q.w = f2h((float)(e[3].x * inv16), (float)(e[3].y * inv16));
+    c16[(size_t)f * V + s] = q;
+    uint2 t;
+    t.x = f2h((float)(e[4].x * inv16), (float)(e[4].y * inv16));
+    t.y = f2h((float)(e[5].x * inv16), (float)(e[5].y * inv16));
+    t16[(size_t)f * V + s] = t;
+  }
+}
+
+template <class T>
+static int dalloc(T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(QEXSTAG_ERR_ALLOC, "device allocation of reduced-precision links failed");
+  }
+  return QEXSTAG_OK;
+}
+
+static int read_uint(unsigned *d, unsigned *h) {
+  QS_CUDA(cudaMemcpyAsync(h, d, sizeof(unsigned), cudaMemcpyDeviceToHost, stream()));
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+static int absmax_links(const double2 *u, size_t n, float *out, unsigned *scratch) {
+  QS_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned), stream()));
+  absmax_kernel<<<grid_for((long)std::min<size_t>(n, 1u << 30)), kBlock, 0, stream()>>>(u, n, scratch);
+  note_launch();
+  QS_LAUNCH_CHECK();
+  unsigned h = 0;
+  int rc = read_uint(scratch, &h);
+  if (rc) return rc;
+  float f;
+  std::memcpy(&f, &h, sizeof(f));
+  *out = f;
+  return QEXSTAG_OK;
+}
+
 int build_low_links(qexstag_links_s *g) {
-  g->low = LowLinks();
-  g->low.nfat = g->nl == 8 ? 4 : 4;
-  g->low.nlong = g->nl == 8 ? 4 : 0;
-  g->low.long_coeff = g->long_coeff;
+  LowLinks &L = g->low;
+  L = LowLinks();
+  const Geom &geo = g->l->g;
+  const size_t V = geo.V;
+  const bool naik = g->nl == 8;
+  L.nfat = 4;
+  L.nlong = naik ? 4 : 0;
+  L.long_coeff = g->long_coeff;
+  unsigned *scratch = (unsigned *)red_tickets() + (kNumTickets - 1);
+  int rc;
+  // scales (max |element|) of the fat and long lists
+  float fat_max = 0.f, long_max = 0.f;
+  for (int k = 0; k < g->nl; k++) {
+    float m = 0.f;
+    if ((rc = absmax_links(g->u64 + (size_t)k * 9 * V, 9 * V, &m, scratch))) return rc;
+    if (naik && (k & 1))
+      long_max = std::max(long_max, m);
+    else
+      fat_max = std::max(fat_max, m);
+  }
+  if (!(fat_max > 0.f) || !std::isfinite(fat_max) || (naik && (!(long_max > 0.f) || !std::isfinite(long_max))))
+    return fail(QEXSTAG_ERR_ARG, "links_create: links are zero or not finite");
+  L.fat_scale = fat_max;
+  L.long_scale = naik ? long_max : 1.0f;
+  // are the long links coeff * sign * SU(3)?
+  if (naik) {
+    QS_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned), stream()));
+    recon_check_kernel<<<grid_for(4L * V), kBlock, 0, stream()>>>(geo, g->u64, g->long_coeff, scratch);
+    note_launch();
+    QS_LAUNCH_CHECK();
+    unsigned h = 0;
+    if ((rc = read_uint(scratch, &h))) return rc;
+    float dev;
+    std::memcpy(&dev, &h, sizeof(dev));
+    L.recon12 = dev < 2e-6f;
+  }
+  if ((rc = dalloc(&L.f32_fat, (size_t)4 * 4 * V)) || (rc = dalloc(&L.f32_fat_tail, (size_t)4 * V)) ||
+      (rc = dalloc(&L.f16_fat, (size_t)4 * 2 * V)) || (rc = dalloc(&L.f16_fat_tail, (size_t)4 * V)))
+    return rc;
+  for (int f = 0; f < 4; f++) {
+    const int k = naik ? 2 * f : f;
+    to_low18_kernel<<<grid_for((long)V), kBlock, 0, stream()>>>(g->u64 + (size_t)k * 9 * V, V, L.f32_fat,
+                                                                L.f32_fat_tail, L.f16_fat, L.f16_fat_tail,
+                                                                f, 1.0f / L.fat_scale);
+    note_launch();
+  }
+  if (naik) {
+    if (L.recon12) {
+      if ((rc = dalloc(&L.f32_long, (size_t)4 * 3 * V)) || (rc = dalloc(&L.f16_long, (size_t)4 * V)) ||
+          (rc = dalloc(&L.f16_long_tail2, (size_t)4 * V)))
+        return rc;
+      for (int f = 0; f < 4; f++) {
+        to_low12_kernel<<<grid_for((long)V), kBlock, 0, stream()>>>(g->u64 + (size_t)(2 * f + 1) * 9 * V, V,
+                                                                    L.f32_long, L.f16_long, L.f16_long_tail2,
+                                                                    f, 1.0f / L.long_scale);
+        note_launch();
+      }
+    } else {
+      if ((rc = dalloc(&L.f32_long, (size_t)4 * 4 * V)) || (rc = dalloc(&L.f32_long_tail, (size_t)4 * V)) ||
+          (rc = dalloc(&L.f16_long, (size_t)4 * 2 * V)) || (rc = dalloc(&L.f16_long_tail, (size_t)4 * V)))
+        return rc;
+      for (int f = 0; f < 4; f++) {
+        to_low18_kernel<<<grid_for((long)V), kBlock, 0, stream()>>>(g->u64 + (size_t)(2 * f + 1) * 9 * V, V,
+                                                                    L.f32_long, L.f32_long_tail, L.f16_long,
+                                                                    L.f16_long_tail, f, 1.0f / L.long_scale);
+        note_launch();
+      }
+    }
+  }
+  QS_LAUNCH_CHECK();
+  L.ready = true;
   return QEXSTAG_OK;
 }
 
@@ -25,20 +230,628 @@ void free_low_links(LowLinks &low) {
   low = LowLinks();
 }
 
+LoLinks lo_links(const LowLinks &low, int prec) {
+  LoLinks L;
+  L.f32_fat = low.f32_fat;
+  L.f32_fat_tail = low.f32_fat_tail;
+  L.f32_long = low.f32_long;
+  L.f32_long_tail = low.f32_long_tail;
+  L.f16_fat = low.f16_fat;
+  L.f16_fat_tail = low.f16_fat_tail;
+  L.f16_long = low.f16_long;
+  L.f16_long_tail2 = low.f16_long_tail2;
+  L.f16_long_tail = low.f16_long_tail;
+  L.recon12 = low.recon12 ? 1 : 0;
+  if (prec == kF16) {
+    L.fat_scale = low.fat_scale;
+    L.long_scale = low.long_scale;
+    L.long_rc = (float)(low.long_scale / low.long_coeff);
+  } else {
+    L.fat_scale = 1.f;
+    L.long_scale = 1.f;
+    L.long_rc = (float)(1.0 / low.long_coeff);
+  }
+  return L;
+}
+
+// ---------------------------------------------------------------------------
+// mixed-precision CG state
+// ---------------------------------------------------------------------------
+
+struct MxState {
+  double r2;     // iterated (sloppy) |r|^2, or the true one after an update
+  double r2old;  // |r|^2 of the previous iteration
+  double alpha, beta, pAp, rp;
+  double b2, r2req, r2stop, delta;
+  double rNorm, r0Norm, maxrx, maxrr;
+  int itn, maxits, done, pending, nan, reliable, pad[2];
+};
+
+__device__ __forceinline__ bool mx_halt(const MxState *st) { return st->done || st->pending; }
+
+// ---------------------------------------------------------------------------
+// sloppy Dslash: out = b*xs + hop * sum_k [...]; fat and long partial sums
+// are kept apart so that the FP16 list scales multiply them once per site.
+// ---------------------------------------------------------------------------
+
+struct DslashArgsLo {
+  Geom g;
+  int po;
+  LoLinks L;
+  const void *xin;
+  int istride;
+  const void *xs;
+  int sstride;
+  void *out;
+  int ostride;
+  float b;
+  const MxState *halt;  // stop when done or pending (may be null)
+  MxState *state;       // pAp finalisation (RED == 1)
+  double *partials;
+  unsigned *ticket;
+  double *dot_out;      // RED == 2
+};
+
+template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
+__global__ void __launch_bounds__(kBlock) dslash_lo_kernel(const DslashArgsLo A) {
+  if (A.halt != nullptr && mx_halt(A.halt)) return;
+  const Geom &g = A.g;
+  const int nh = g.nh;
+  const size_t V = (size_t)g.V;
+  const size_t in_base = (size_t)(1 - A.po) * nh;
+  const size_t out_base = (size_t)A.po * nh;
+  double dot = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+    int x[4], lex;
+    site_coords(g, A.po, k, x, lex);
+    float2 af[3], al[3], xsv[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      af[c] = make_float2(0.f, 0.f);
+      al[c] = make_float2(0.f, 0.f);
+    }
+    if (INIT) load_vec_cg<PREC>(A.xs, A.sstride, k, xsv);
+#pragma unroll
+    for (int l = 0; l < NL; l++) {
+      const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
+      const bool is_long = (NL == 8) && (l & 1);
+      const int f = (NL == 8) ? (l >> 1) : l;
+      const int jf = nbr_half(g, x, lex, mu, len);
+      const int jb = nbr_half(g, x, lex, mu, -len);
+      float2 v[3], w[3], uf[9], ub[9];
+      load_vec<PREC>(A.xin, A.istride, jf, v);
+      load_vec<PREC>(A.xin, A.istride, jb, w);
+      if (is_long) {
+        if (R12) {
+          load_long12<PREC>(A.L, f, out_base + k, V, long_sign_fwd(g, x, mu), uf);
+          load_long12<PREC>(A.L, f, in_base + jb, V, long_sign_bck(g, x, mu), ub);
+        } else {
+          load_link18<PREC>(A.L.f32_long, A.L.f32_long_tail, A.L.f16_long, A.L.f16_long_tail, f,
+                            out_base + k, V, uf);
+          load_link18<PREC>(A.L.f32_long, A.L.f32_long_tail, A.L.f16_long, A.L.f16_long_tail, f,
+                            in_base + jb, V, ub);
+        }
+      } else {
+        load_link18<PREC>(A.L.f32_fat, A.L.f32_fat_tail, A.L.f16_fat, A.L.f16_fat_tail, f, out_base + k,
+                          V, uf);
+        load_link18<PREC>(A.L.f32_fat, A.L.f32_fat_tail, A.L.f16_fat, A.L.f16_fat_tail, f, in_base + jb,
+                          V, ub);
+      }
+      float2 t[3], q[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        t[i] = make_float2(0.f, 0.f);
+        q[i] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          t[i] = cmadd(t[i], uf[3 * i + j], v[j]);
+          q[i] = cjmadd(q[i], ub[3 * j + i], w[j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        float2 d = make_float2(t[i].x - q[i].x, t[i].y - q[i].y);
+        if (is_long) {
+          al[i].x += d.x;
+          al[i].y += d.y;
+        } else {
+          af[i].x += d.x;
+          af[i].y += d.y;
+        }
+      }
+    }
+    float2 o[3];
+    const float sf = HOP > 0 ? A.L.fat_scale : -A.L.fat_scale;
+    const float sl = HOP > 0 ? A.L.long_scale : -A.L.long_scale;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 acc = INIT ? make_float2(A.b * xsv[c].x, A.b * xsv[c].y) : make_float2(0.f, 0.f);
+      acc.x = fmaf(sf, af[c].x, acc.x);
+      acc.y = fmaf(sf, af[c].y, acc.y);
+      if (NL == 8) {
+        acc.x = fmaf(sl, al[c].x, acc.x);
+        acc.y = fmaf(sl, al[c].y, acc.y);
+      }
+      o[c] = acc;
+    }
+    store_vec<OUTP>(A.out, A.ostride, k, o);
+    if (RED) {
+      float d = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; c++) d += xsv[c].x * o[c].x + xsv[c].y * o[c].y;
+      dot += (double)d;
+    }
+  }
+  if (RED) {
+    double v[1] = {dot}, s[1];
+    if (grid_reduce<1>(v, A.partials, A.ticket, s) && threadIdx.x == 0) {
+      if (RED == 1) {
+        MxState *st = A.state;
+        st->pAp = s[0];
+        st->alpha = st->r2 / s[0];
+        st->itn += 1;
+      } else {
+        *A.dot_out = s[0];
+      }
+    }
+  }
+}
+
+template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP>
+static void launch_lo(const DslashArgsLo &A, int grid) {
+  if (NL == 8 && A.L.recon12)
+    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 1><<<grid, kBlock, 0, stream()>>>(A);
+  else
+    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 0><<<grid, kBlock, 0, stream()>>>(A);
+  note_launch();
+}
+
+// the two half sweeps of the sloppy Schur operator:
+//   which 0: t = (2D)_{q,par} p                (out: PREC, hop +1)
+//   which 1: ap = 4 m2 p - (2D)_{par,q} t      (out: FP32, hop -1, pAp)
+template <int PREC, int NL>
+static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red) {
+  if (which == 0) {
+    launch_lo<PREC, NL, 1, 0, 0, PREC>(A, grid);
+  } else if (red == 1) {
+    launch_lo<PREC, NL, -1, 1, 1, kF32>(A, grid);
+  } else if (red == 2) {
+    launch_lo<PREC, NL, -1, 1, 2, kF32>(A, grid);
+  } else {
+    launch_lo<PREC, NL, -1, 1, 0, kF32>(A, grid);
+  }
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
+// sloppy Schur: ap (FP32 [3][nh]) = 4 m2 p - (2D)(2D) p on parity par,
+// p and t in format prec.
+int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void *p, void *t,
+             double m2, int red, MxState *state, const MxState *halt, double *dot_out) {
+  const Geom &geo = g->l->g;
+  DslashArgsLo A;
+  A.g = geo;
+  A.L = lo_links(g->low, prec);
+  A.halt = halt;
+  A.state = state;
+  A.partials = red_partials();
+  A.ticket = red_tickets();
+  A.dot_out = dot_out;
+  int grid = grid_for(geo.nh, kBlock, 6);
+  if (grid > kMaxRedBlocks) grid = kMaxRedBlocks;
+  // half sweep 1
+  A.po = 1 - par;
+  A.xin = p;
+  A.istride = geo.nh;
+  A.xs = nullptr;
+  A.sstride = 0;
+  A.out = t;
+  A.ostride = geo.nh;
+  A.b = 0.f;
+  int rc;
+  if (prec == kF32)
+    rc = g->nl == 8 ? sloppy_half<kF32, 8>(0, A, grid, 0) : sloppy_half<kF32, 4>(0, A, grid, 0);
+  else
+    rc = g->nl == 8 ? sloppy_half<kF16, 8>(0, A, grid, 0) : sloppy_half<kF16, 4>(0, A, grid, 0);
+  if (rc) return rc;
+  // half sweep 2
+  A.po = par;
+  A.xin = t;
+  A.xs = p;
+  A.sstride = geo.nh;
+  A.out = ap;
+  A.b = (float)(4.0 * m2);
+  if (prec == kF32)
+    rc = g->nl == 8 ? sloppy_half<kF32, 8>(1, A, grid, red) : sloppy_half<kF32, 4>(1, A, grid, red);
+  else
+    rc = g->nl == 8 ? sloppy_half<kF16, 8>(1, A, grid, red) : sloppy_half<kF16, 4>(1, A, grid, red);
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// mixed CG kernels
+// ---------------------------------------------------------------------------
+
+template <int PREC>
+__global__ void __launch_bounds__(kBlock)
+    mx_init_kernel(const double2 *__restrict__ b, int bs, double2 *__restrict__ x, double2 *__restrict__ r,
+                   float2 *__restrict__ rs, float2 *__restrict__ xs, void *p, int n, MxState *st,
+                   double *partials, unsigned *ticket) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double2 v = b[(size_t)c * bs + i];
+      x[(size_t)c * n + i] = make_double2(0.0, 0.0);
+      r[(size_t)c * n + i] = v;
+      pv[c] = make_float2((float)v.x, (float)v.y);
+      rs[(size_t)c * n + i] = pv[c];
+      xs[(size_t)c * n + i] = make_float2(0.f, 0.f);
+      s = fma(v.x, v.x, s);
+      s = fma(v.y, v.y, s);
+    }
+    store_vec<PREC>(p, n, i, pv);
+  }
+  double v[1] = {s}, o[1];
+  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) {
+    double b2 = o[0];
+    st->b2 = b2;
+    st->r2 = b2;
+    st->r2old = b2;
+    st->r2stop = st->r2req * b2;
+    st->rNorm = st->r0Norm = st->maxrx = st->maxrr = sqrt(b2);
+    st->itn = 0;
+    st->pending = 0;
+    st->reliable = 0;
+    st->nan = isfinite(b2) ? 0 : 1;
+    st->done = (!(b2 > st->r2stop) || st->maxits <= 0 || st->nan) ? 1 : 0;
+  }
+}
+
+// rs -= alpha ap; xs += alpha p; then the reliable-update decision
+template <int PREC>
+__global__ void __launch_bounds__(kBlock)
+    mx_update_kernel(float2 *__restrict__ rs, float2 *__restrict__ xs, const float2 *__restrict__ ap,
+                     const void *p, int n, MxState *st, double *partials, unsigned *ticket) {
+  if (mx_halt(st)) return;
+  const float alpha = (float)st->alpha;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+    load_vec<PREC>(p, n, i, pv);
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 r = rs[(size_t)c * n + i], a = ap[(size_t)c * n + i], xv = xs[(size_t)c * n + i];
+      r.x = fmaf(-alpha, a.x, r.x);
+      r.y = fmaf(-alpha, a.y, r.y);
+      xv.x = fmaf(alpha, pv[c].x, xv.x);
+      xv.y = fmaf(alpha, pv[c].y, xv.y);
+      rs[(size_t)c * n + i] = r;
+      xs[(size_t)c * n + i] = xv;
+      acc = fmaf(r.x, r.x, acc);
+      acc = fmaf(r.y, r.y, acc);
+    }
+    s += (double)acc;
+  }
+  double v[1] = {s}, o[1];
+  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) {
+    const double r2 = o[0];
+    st->r2old = st->r2;
+    st->r2 = r2;
+    if (!isfinite(r2)) {
+      st->nan = 1;
+      st->done = 1;
+      return;
+    }
+    const double rn = sqrt(r2);
+    st->rNorm = rn;
+    st->maxrr = fmax(st->maxrr, rn);
+    st->maxrx = fmax(st->maxrx, rn);
+    const bool ux = rn < st->delta * st->r0Norm && st->r0Norm <= st->maxrx;
+    const bool ur = (rn < st->delta * st->maxrr && st->r0Norm <= st->maxrr) || ux;
+    if (ur || r2 <= st->r2stop || st->itn >= st->maxits) {
+      st->pending = 1;
+    } else {
+      st->beta = r2 / st->r2old;
+    }
+  }
+}
+
+template <int PREC>
+__global__ void mx_p_kernel(const float2 *__restrict__ rs, void *p, int n, const MxState *st) {
+  if (mx_halt(st)) return;
+  const float beta = (float)st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+    load_vec_cg<PREC>(p, n, i, pv);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 r = rs[(size_t)c * n + i];
+      pv[c] = make_float2(fmaf(beta, pv[c].x, r.x), fmaf(beta, pv[c].y, r.y));
+    }
+    store_vec<PREC>(p, n, i, pv);
+  }
+}
+
+// reliable update part 1: x += xs, xs = 0
+__global__ void mx_flush_kernel(double2 *__restrict__ x, float2 *__restrict__ xs, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) {
+    float2 v = xs[i];
+    double2 w = x[i];
+    w.x += (double)v.x;
+    w.y += (double)v.y;
+    x[i] = w;
+    xs[i] = make_float2(0.f, 0.f);
+  }
+}
+
+// reliable update part 2: r = b - Ax (FP64), rs = r, true |r|^2 and decisions
+__global__ void __launch_bounds__(kBlock)
+    mx_true_res_kernel(const double2 *__restrict__ b, int bs, const double2 *__restrict__ ax,
+                       double2 *__restrict__ r, float2 *__restrict__ rs, int n, MxState *st,
+                       double *partials, unsigned *ticket) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double2 bv = b[(size_t)c * bs + i], a = ax[(size_t)c * n + i];
+      double2 v = make_double2(bv.x - a.x, bv.y - a.y);
+      r[(size_t)c * n + i] = v;
+      rs[(size_t)c * n + i] = make_float2((float)v.x, (float)v.y);
+      s = fma(v.x, v.x, s);
+      s = fma(v.y, v.y, s);
+    }
+  }
+  double v[1] = {s}, o[1];
+  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) {
+    const double r2 = o[0];
+    st->r2 = r2;
+    st->reliable += 1;
+    if (!isfinite(r2)) {
+      st->nan = 1;
+      st->done = 1;
+      return;
+    }
+    if (r2 <= st->r2stop || st->itn >= st->maxits) {
+      st->done = 1;
+      return;
+    }
+    const double rn = sqrt(r2);
+    st->rNorm = st->r0Norm = st->maxrr = st->maxrx = rn;
+    st->beta = r2 / st->r2old;
+  }
+}
+
+// reliable update part 3: rp = <rs, p>
+template <int PREC>
+__global__ void __launch_bounds__(kBlock)
+    mx_rp_kernel(const float2 *__restrict__ rs, const void *p, int n, MxState *st, double *partials,
+                 unsigned *ticket) {
+  if (st->done) return;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+    load_vec<PREC>(p, n, i, pv);
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 r = rs[(size_t)c * n + i];
+      acc = fmaf(r.x, pv[c].x, acc);
+      acc = fmaf(r.y, pv[c].y, acc);
+    }
+    s += (double)acc;
+  }
+  double v[1] = {s}, o[1];
+  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) st->rp = o[0];
+}
+
+// reliable update part 4: p = rs + beta (p - (rp/r2) rs); clears pending
+template <int PREC>
+__global__ void mx_p_reliable_kernel(const float2 *__restrict__ rs, void *p, int n, MxState *st) {
+  if (st->done) return;
+  const float beta = (float)st->beta;
+  const float g = (float)(st->rp / st->r2);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+    load_vec_cg<PREC>(p, n, i, pv);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 r = rs[(size_t)c * n + i];
+      float2 q = make_float2(fmaf(-g, r.x, pv[c].x), fmaf(-g, r.y, pv[c].y));
+      pv[c] = make_float2(fmaf(beta, q.x, r.x), fmaf(beta, q.y, r.y));
+    }
+    store_vec<PREC>(p, n, i, pv);
+  }
+}
+
+__global__ void mx_clear_pending_kernel(MxState *st) { st->pending = 0; }
+
+int read_mx(const MxState *d, MxState *h) {
+  double *buf = host_results();
+  static_assert(sizeof(MxState) <= sizeof(double) * kNumResults, "state too large");
+  QS_CUDA(cudaMemcpyAsync(buf, d, sizeof(MxState), cudaMemcpyDeviceToHost, stream()));
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  std::memcpy(h, buf, sizeof(MxState));
+  return QEXSTAG_OK;
+}
+
+int check_interval(int nh);
+
+template <int PREC>
+static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req,
+                      int maxits, double delta, CgOut *out, int *reliable) {
+  const Geom &geo = g->l->g;
+  const int nh = geo.nh;
+  Workspace &ws = g->ws;
+  const size_t v64 = sizeof(double2) * 3 * (size_t)nh, v32 = sizeof(float2) * 3 * (size_t)nh;
+  const size_t vp = (PREC == kF32) ? v32 : sizeof(uint4) * (size_t)nh;
+  void *pr, *pax, *prs, *pxs, *pap, *pp, *pt, *pt64, *pst;
+  int rc;
+  if ((rc = ws.get(kSlotMx0 + 0, v64, &pr)) || (rc = ws.get(kSlotMx0 + 1, v64, &pax)) ||
+      (rc = ws.get(kSlotMx0 + 2, v32, &prs)) || (rc = ws.get(kSlotMx0 + 3, v32, &pxs)) ||
+      (rc = ws.get(kSlotMx0 + 4, v32, &pap)) || (rc = ws.get(kSlotMx0 + 5 + 2 * PREC, vp, &pp)) ||
+      (rc = ws.get(kSlotMx0 + 6 + 2 * PREC, vp, &pt)) || (rc = ws.get(kSlotMx0 + 9, v64, &pt64)) ||
+      (rc = ws.get(kSlotMx0 + 10, sizeof(MxState), &pst)))
+    return rc;
+  double2 *r = (double2 *)pr, *ax = (double2 *)pax;
+  float2 *rs = (float2 *)prs, *xs = (float2 *)pxs, *ap = (float2 *)pap;
+  MxState *st = (MxState *)pst;
+  MxState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.r2req = r2req;
+  hs.maxits = maxits;
+  hs.delta = delta;
+  {
+    double *buf = host_results();
+    std::memcpy(buf, &hs, sizeof(hs));
+    QS_CUDA(cudaMemcpyAsync(st, buf, sizeof(hs), cudaMemcpyHostToDevice, stream()));
+  }
+  const int grid = grid_for(nh, kBlock, 4);
+  const int egrid = grid_for(nh, kBlock, 8);
+  mx_init_kernel<PREC><<<grid, kBlock, 0, stream()>>>(b.p, b.stride, x.p, r, rs, xs, pp, nh, st,
+                                                      red_partials(), red_tickets());
+  note_launch();
+  QS_LAUNCH_CHECK();
+  const int every = check_interval(nh);
+  for (;;) {
+    for (int i = 0; i < every; i++) {
+      if ((rc = schur_lo(g, PREC, par, ap, pp, pt, m2, 1, st, st, nullptr))) return rc;
+      mx_update_kernel<PREC><<<grid, kBlock, 0, stream()>>>(rs, xs, ap, pp, nh, st, red_partials(),
+                                                            red_tickets());
+      mx_p_kernel<PREC><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
+      note_launch(2);
+    }
+    QS_LAUNCH_CHECK();
+    if ((rc = read_mx(st, &hs))) return rc;
+    if (hs.done) break;
+    if (!hs.pending) continue;
+    // reliable update: fold the increment in, FP64 true residual
+    mx_flush_kernel<<<egrid, kBlock, 0, stream()>>>(x.p, xs, nh);
+    note_launch();
+    if ((rc = schur64(g, par, VecD{ax, nh}, cv(x), VecD{(double2 *)pt64, nh}, m2))) return rc;
+    mx_true_res_kernel<<<grid, kBlock, 0, stream()>>>(b.p, b.stride, ax, r, rs, nh, st, red_partials(),
+                                                      red_tickets());
+    mx_rp_kernel<PREC><<<grid, kBlock, 0, stream()>>>(rs, pp, nh, st, red_partials(), red_tickets());
+    mx_p_reliable_kernel<PREC><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
+    mx_clear_pending_kernel<<<1, 1, 0, stream()>>>(st);
+    note_launch(4);
+    QS_LAUNCH_CHECK();
+    if ((rc = read_mx(st, &hs))) return rc;
+    if (hs.done) break;
+  }
+  out->iterations = hs.itn;
+  out->r2 = hs.b2 > 0 ? hs.r2 / hs.b2 : 0.0;
+  out->nan = hs.nan;
+  *reliable = hs.reliable;
+  if (hs.nan) return fail(QEXSTAG_ERR_NAN, "mixed cg: NaN in residual");
+  return QEXSTAG_OK;
+}
+
 int cg_mixed(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, int maxits,
              int sloppy, double delta, CgOut *out, int *reliable) {
-  return fail(QEXSTAG_ERR_ARG, "sloppy solves are not available in this build");
-}
-
-int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nrhs,
-           const double2 *const *b, double2 *const *y, const qexstag_solver_params *p,
-           qexstag_solver_stats *st, double *r2_out) {
-  return fail(QEXSTAG_ERR_ARG, "cgm_ee is not available in this build");
-}
-
-int solve_multishift(qexstag_links_s *g, int nmass, double2 *const *xs, const double2 *b,
-                     const double *ms, const qexstag_solver_params *p, qexstag_solver_stats *st) {
-  return fail(QEXSTAG_ERR_ARG, "solve_multishift is not available in this build");
+  if (!g->low.ready) return fail(QEXSTAG_ERR_STATE, "reduced-precision links missing");
+  if (x.stride != g->l->g.V && x.stride != g->l->g.nh)
+    return fail(QEXSTAG_ERR_ARG, "cg_mixed: bad solution stride");
+  // the solution accumulates in a compact [3][nh] buffer, copied out at the end
+  const int nh = g->l->g.nh;
+  void *px;
+  int rc = g->ws.get(kSlotMx0 + 11, sizeof(double2) * 3 * (size_t)nh, &px);
+  if (rc) return rc;
+  VecD xc{(double2 *)px, nh};
+  rc = (sloppy == QEXSTAG_SLOPPY_HALF) ? cg_mixed_t<kF16>(g, par, m2, b, xc, r2req, maxits, delta, out, reliable)
+                                       : cg_mixed_t<kF32>(g, par, m2, b, xc, r2req, maxits, delta, out, reliable);
+  if (rc) return rc;
+  return vcopy(x, cv(xc), nh);
 }
 
 }  // namespace qs
+
+// ---------------------------------------------------------------------------
+// timing of the Schur operator in each precision (benchmark hook)
+// ---------------------------------------------------------------------------
+namespace qs {
+
+template <int PREC>
+__global__ void fill_vec_kernel(void *p, int n, unsigned seed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 v[3];
+    unsigned h = (unsigned)i * 2654435761u + seed;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      h ^= h >> 13;
+      h *= 0x5bd1e995u;
+      float a = (float)(h & 0xffff) * (1.f / 65536.f) - 0.5f;
+      h ^= h >> 15;
+      h *= 0x27d4eb2du;
+      float b = (float)(h & 0xffff) * (1.f / 65536.f) - 0.5f;
+      v[c] = make_float2(a, b);
+    }
+    store_vec<PREC>(p, n, i, v);
+  }
+}
+
+__global__ void fill_vec64_kernel(double2 *p, int n, unsigned seed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) {
+    unsigned h = (unsigned)i * 2654435761u + seed;
+    h ^= h >> 13;
+    h *= 0x5bd1e995u;
+    p[i] = make_double2((double)(h & 0xffff) / 65536.0 - 0.5, (double)((h >> 16) & 0xffff) / 65536.0 - 0.5);
+  }
+}
+
+int bench_schur(qexstag_links_s *g, int prec, int nrep, double m2, double *sec) {
+  const Geom &geo = g->l->g;
+  const int nh = geo.nh;
+  Workspace &ws = g->ws;
+  void *pa, *pb, *pc;
+  int rc;
+  const size_t v64 = sizeof(double2) * 3 * (size_t)nh;
+  if ((rc = ws.get(kSlotMx0 + 20, v64, &pa)) || (rc = ws.get(kSlotMx0 + 21, v64, &pb)) ||
+      (rc = ws.get(kSlotMx0 + 22, v64, &pc)))
+    return rc;
+  const int grid = grid_for(nh);
+  if (prec == 0) {
+    fill_vec64_kernel<<<grid, kBlock, 0, stream()>>>((double2 *)pa, nh, 1u);
+  } else if (prec == 1) {
+    fill_vec_kernel<kF32><<<grid, kBlock, 0, stream()>>>(pa, nh, 1u);
+  } else {
+    fill_vec_kernel<kF16><<<grid, kBlock, 0, stream()>>>(pa, nh, 1u);
+  }
+  note_launch();
+  QS_LAUNCH_CHECK();
+  auto once = [&]() -> int {
+    if (prec == 0)
+      return schur64(g, 0, VecD{(double2 *)pc, nh}, CVecD{(const double2 *)pa, nh}, VecD{(double2 *)pb, nh}, m2);
+    return schur_lo(g, prec == 1 ? kF32 : kF16, 0, (float2 *)pc, pa, pb, m2, 0, nullptr, nullptr, nullptr);
+  };
+  for (int i = 0; i < 2; i++)
+    if ((rc = once())) return rc;
+  cudaEvent_t e0, e1;
+  QS_CUDA(cudaEventCreate(&e0));
+  QS_CUDA(cudaEventCreate(&e1));
+  QS_CUDA(cudaEventRecord(e0, stream()));
+  for (int i = 0; i < nrep; i++)
+    if ((rc = once())) break;
+  cudaEventRecord(e1, stream());
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  *sec = ms * 1e-3 / nrep;
+  return QEXSTAG_OK;
+}
+
+}  // namespace qs
+
+extern "C" int qexstag_bench_schur(qexstag_links *g, int prec, int nrep, double m2,
+                                   double *seconds_per_call) {
+  if (!g || !g->u64 || !seconds_per_call || nrep < 1 || prec < 0 || prec > 2)
+    return qs::fail(QEXSTAG_ERR_ARG, "bench_schur: bad argument");
+  int rc = qs::runtime_ready();
+  if (rc) return rc;
+  return qs::bench_schur(g, prec, nrep, m2, seconds_per_call);
+}

@@ -273,6 +273,14 @@ class Staggered:
         sp.take(st, rc)
         return r2.reshape(nrhs, nsh)
 
+    def bench_schur(self, prec: int, nrep: int = 20, m2: float = 1e-4) -> float:
+        """Seconds per even-parity Schur operator call in precision prec
+        (0 FP64, 1 FP32, 2 FP16), timed with CUDA events in the library."""
+        out = C.c_double()
+        L.check(self._lib.qexstag_bench_schur(self.handle, prec, nrep, m2, C.byref(out)),
+                "bench_schur")
+        return out.value
+
     # ---- force ----
     def force(self, f, phi, m: float, sp: SolverParams) -> None:
         """stagForceSolve + fermForce (no smearing): f receives the force QEX

@@ -149,3 +149,73 @@ def test_force_matches_oracle(cuda, naik):
     o.ferm_force(fo2, psi)
     s.ferm_force(fg2, psi)
     assert rel(fg2, fo2) < 1e-13
+
+
+@pytest.mark.parametrize("sloppy", [L.SLOPPY_SINGLE, L.SLOPPY_HALF])
+@pytest.mark.parametrize("naik", [False, True])
+def test_mixed_precision_solveEE(cuda, naik, sloppy):
+    """Reliable-update FP32/FP16 inner CG inside FP64 defect correction
+    reaches the FP64 true residual and agrees with the FP64 oracle solve."""
+    dims = (8, 8, 8, 8)
+    V = F.volume(dims)
+    g = links_for(dims, naik)
+    m = 0.05
+    o = O.Oracle(dims, g)
+    s = S.Staggered(S.Layout(dims), g)
+    if naik:
+        assert s.recon12
+    b = F.even_source(dims, 61)
+    yo = o.vec()
+    o.solveXX(0, yo, b, m, 1e-22)
+    y = o.vec()
+    sp = S.SolverParams(r2req=1e-20, sloppySolve=sloppy)
+    s.solveEE(y, b, m, sp)
+    assert sp.status == L.OK
+    assert true_r2_ee(o, y, b, m) <= 1e-20
+    assert rel(y, yo) < 1e-8
+    assert sp.reliable_updates >= 1
+
+
+def test_mixed_without_recon12(cuda):
+    """Long links that are not a phase times SU(3) keep all 18 reals."""
+    dims = (8, 8, 8, 8)
+    g = links_for(dims, True)
+    g[1::2] = g[0::2] * 0.5  # long := half the fat links (not unitary)
+    o = O.Oracle(dims, g)
+    s = S.Staggered(S.Layout(dims), g)
+    assert not s.recon12
+    b = F.even_source(dims, 62)
+    for sloppy in (L.SLOPPY_SINGLE, L.SLOPPY_HALF):
+        y = o.vec()
+        s.solveEE(y, b, 0.1, S.SolverParams(r2req=1e-20, sloppySolve=sloppy))
+        assert true_r2_ee(o, y, b, 0.1) <= 1e-20
+
+
+def test_mixed_long_coeff(cuda):
+    """A long-link coefficient (QEX HISQ folds naik = -1/24 into the long
+    links) is honoured by the 12-real reconstruction."""
+    dims = (8, 8, 8, 8)
+    g = links_for(dims, True)
+    c = -1.0 / 24.0
+    g[1::2] *= c
+    o = O.Oracle(dims, g)
+    s = S.Staggered(S.Layout(dims), g, long_coeff=c)
+    assert s.recon12
+    b = F.even_source(dims, 63)
+    y = o.vec()
+    s.solveEE(y, b, 0.05, S.SolverParams(r2req=1e-20, sloppySolve=L.SLOPPY_HALF))
+    assert true_r2_ee(o, y, b, 0.05) <= 1e-20
+
+
+def test_mixed_full_solve(cuda):
+    dims = (8, 8, 8, 8)
+    V = F.volume(dims)
+    g = links_for(dims, True)
+    o = O.Oracle(dims, g)
+    s = S.Staggered(S.Layout(dims), g)
+    b = F.gaussian_vector(V, 64)
+    x = o.vec()
+    s.solve(x, b, 0.1, S.SolverParams(r2req=1e-20, sloppySolve=L.SLOPPY_HALF))
+    dx = o.vec()
+    o.D(dx, x, 0.1)
+    assert np.linalg.norm(dx - b) ** 2 / np.linalg.norm(b) ** 2 <= 1e-20
