@@ -1,0 +1,64 @@
+"""Time the even-parity Schur operator (two Dslash half sweeps) per precision
+and report HBM throughput against its compulsory bytes.
+
+  python -m qex_b200.kernel_timing [--dims 32,32,32,32] [--naive]
+                                   [--prec 0,1,2] [--nrep 20]
+
+Compulsory bytes per even site of one Schur application (each link read
+once per half sweep, each vector once; 12-real long links):
+  FP64 fat+Naik  2400 + 2448 = 4848     naive 1248 + 1296 = 2544
+  FP32 fat+Naik  1008 + 1032 = 2040     naive  624 +  648 = 1272
+  FP16 fat+Naik   512 +  536 = 1048     naive  320 +  344 =  664
+(second half sweep: + same-site input and an FP32 output for the sloppy
+precisions).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+BYTES = {  # (nlinks, prec) -> bytes per even site per Schur call
+    (8, 0): 4848, (8, 1): 2040, (8, 2): 1048,
+    (4, 0): 2544, (4, 1): 1272, (4, 2): 664,
+}
+NAMES = {0: "fp64", 1: "fp32", 2: "fp16"}
+
+
+def bytes_per_site(nlinks: int, prec: int, recon12: bool = True) -> int:
+    b = BYTES[(nlinks, prec)]
+    if nlinks == 8 and prec > 0 and not recon12:
+        b += 2 * 4 * (2 * 24 if prec == 1 else 2 * 12)  # long links with 18 reals
+    return b
+
+
+def time_schur(stag, nh: int, precs=(0, 1, 2), nrep: int = 20, m2: float = 1e-4):
+    out = {}
+    for p in precs:
+        sec = stag.bench_schur(p, nrep, m2)
+        bps = bytes_per_site(stag.nlinks, p, stag.recon12)
+        out[NAMES[p]] = {"seconds": sec, "bytes_per_even_site": bps,
+                         "GBps": bps * nh / sec / 1e9,
+                         "GFLOPs": (2 * (1146 if stag.nlinks == 8 else 570)) * nh / sec / 1e9}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dims", default="32,32,32,32")
+    ap.add_argument("--naive", action="store_true")
+    ap.add_argument("--prec", default="0,1,2")
+    ap.add_argument("--nrep", type=int, default=20)
+    a = ap.parse_args()
+    from . import fields as F
+    from . import stag as S
+    dims = tuple(int(v) for v in a.dims.split(","))
+    S.init(0)
+    g = F.naive_links(dims) if a.naive else F.fat_naik_links(dims)
+    s = S.Staggered(S.Layout(dims), S.to_device_links(g))
+    del g
+    res = time_schur(s, F.volume(dims) // 2, [int(v) for v in a.prec.split(",")], a.nrep)
+    print(json.dumps({"dims": dims, "nlinks": s.nlinks, "recon12": s.recon12, "schur": res}))
+
+
+if __name__ == "__main__":
+    main()
