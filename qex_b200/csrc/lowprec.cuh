@@ -10,15 +10,22 @@
 namespace qs {
 
 constexpr int kF32 = 0;
-constexpr int kF16 = 1;
+constexpr int kF16 = 1;  // 16-bit fixed point (see h2f)
 
+// 16-bit storage is fixed point: a signed 16-bit integer per real, scaled
+// by a per-site norm (colour vectors) or a per-list scale (links) so that
+// the largest magnitude maps to 32767.  This keeps 15 bits of resolution
+// relative to the largest element, where an IEEE half keeps 11.
+constexpr float kI16 = 32767.f;
+// raw integers of a packed pair, as floats (no scaling)
 __device__ __forceinline__ float2 h2f(unsigned u) {
-  __half2 h = *reinterpret_cast<__half2 *>(&u);
-  return __half22float2(h);
+  return make_float2((float)(short)(u & 0xffffu), (float)(short)(u >> 16));
 }
+// pack two values in [-1, 1]
 __device__ __forceinline__ unsigned f2h(float a, float b) {
-  __half2 h = __floats2half2_rn(a, b);
-  return *reinterpret_cast<unsigned *>(&h);
+  int ia = __float2int_rn(fminf(fmaxf(a, -1.f), 1.f) * kI16);
+  int ib = __float2int_rn(fminf(fmaxf(b, -1.f), 1.f) * kI16);
+  return ((unsigned)ia & 0xffffu) | (((unsigned)ib & 0xffffu) << 16);
 }
 
 // Link pointers of one handle as the kernels see them.
@@ -32,9 +39,9 @@ struct LoLinks {
   const uint4 *f16_long;
   const uint2 *f16_long_tail2;
   const unsigned *f16_long_tail;
-  float fat_scale;   // FP16 value scale of fat (or naive) links; 1 for FP32
-  float long_scale;  // FP16 value scale of long links; 1 for FP32
-  float long_rc;     // row-2 factor of a 12-real long link: scale / long_coeff
+  float fat_scale;   // value of one raw 16-bit unit of fat (or naive) links; 1 for FP32
+  float long_scale;  // value of one raw 16-bit unit of long links; 1 for FP32
+  float long_rc;     // row-2 factor of a 12-real long link: long_scale / long_coeff
   int recon12;
 };
 
@@ -120,7 +127,7 @@ __device__ __forceinline__ void load_long12(const LoLinks &L, int f, size_t site
   recon_row2(u, s * L.long_rc);
 }
 
-// colour vectors: FP32 float2[3][stride]; FP16 uint4[stride]
+// colour vectors: FP32 float2[3][stride]; 16-bit uint4[stride]
 template <int PREC>
 __device__ __forceinline__ void load_vec(const void *base, int stride, int i, float2 v[3]) {
   if (PREC == kF32) {
@@ -129,7 +136,7 @@ __device__ __forceinline__ void load_vec(const void *base, int stride, int i, fl
     for (int c = 0; c < 3; c++) v[c] = ldg(p + (size_t)c * stride + i);
   } else {
     uint4 q = ldg((const uint4 *)base + i);
-    float n = __uint_as_float(q.w);
+    float n = __uint_as_float(q.w) * (1.f / kI16);
     float2 a = h2f(q.x), b = h2f(q.y), c = h2f(q.z);
     v[0] = make_float2(n * a.x, n * a.y);
     v[1] = make_float2(n * b.x, n * b.y);
@@ -145,7 +152,7 @@ __device__ __forceinline__ void load_vec_cg(const void *base, int stride, int i,
     for (int c = 0; c < 3; c++) v[c] = __ldcg(p + (size_t)c * stride + i);
   } else {
     uint4 q = __ldcg((const uint4 *)base + i);
-    float n = __uint_as_float(q.w);
+    float n = __uint_as_float(q.w) * (1.f / kI16);
     float2 a = h2f(q.x), b = h2f(q.y), c = h2f(q.z);
     v[0] = make_float2(n * a.x, n * a.y);
     v[1] = make_float2(n * b.x, n * b.y);

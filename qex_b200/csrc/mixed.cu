@@ -243,9 +243,9 @@ LoLinks lo_links(const LowLinks &low, int prec) {
   L.f16_long_tail = low.f16_long_tail;
   L.recon12 = low.recon12 ? 1 : 0;
   if (prec == kF16) {
-    L.fat_scale = low.fat_scale;
-    L.long_scale = low.long_scale;
-    L.long_rc = (float)(low.long_scale / low.long_coeff);
+    L.fat_scale = low.fat_scale / kI16;
+    L.long_scale = low.long_scale / kI16;
+    L.long_rc = (float)((double)low.long_scale / kI16 / low.long_coeff);
   } else {
     L.fat_scale = 1.f;
     L.long_scale = 1.f;

@@ -4,12 +4,15 @@
 //
 //  FP32 link, 18 reals:   float4 [n][4][V] (elements 0..7) + float2 [n][V] (element 8)
 //  FP32 long link, 12 reals (rows 0 and 1): float4 [n][3][V]
-//  FP16 link, 18 reals:   uint4 [n][2][V] (elements 0..7 as half2) + unsigned [n][V]
-//                          (element 8); value = half * scale (one scale per list)
-//  FP16 long link, 12 reals: uint4 [n][V] (elements 0..3) + uint2 [n][V] (4..5)
+//  16-bit link, 18 reals: uint4 [n][2][V] (elements 0..7, one re/im pair of
+//                          int16 per 32-bit word) + unsigned [n][V] (element 8);
+//                          value = int16 / 32767 * scale, scale = max |real| of the list
+//  16-bit long link, 12 reals: uint4 [n][V] (elements 0..3) + uint2 [n][V] (4..5)
 //  FP32 vector:           float2 [3][stride]
-//  FP16 vector:           uint4 [stride] = (half2 c0, half2 c1, half2 c2, float norm),
-//                          value = half * norm, norm = max |real| of the site
+//  16-bit vector:         uint4 [stride] = (c0, c1, c2 as int16 re/im pairs, float norm),
+//                          value = int16 / 32767 * norm, norm = max |real| of the site
+// The 16-bit formats are what the API calls half precision (SLOPPY_HALF):
+// 16-bit fixed point with FP32 scales, computed in FP32.
 //
 // A 12-real long link stores rows 0 and 1 of W = s*c*U, U in SU(3), s = +-1 the
 // folded phase/boundary sign of that link and c the long-link coefficient.

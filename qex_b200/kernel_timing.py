@@ -48,6 +48,9 @@ def main():
     ap.add_argument("--naive", action="store_true")
     ap.add_argument("--prec", default="0,1,2")
     ap.add_argument("--nrep", type=int, default=20)
+    ap.add_argument("--solve", type=int, default=-1,
+                    help="instead: one warm-up and one timed solveEE (m=0.01, r2req 1e-20) "
+                         "with this inner precision (0 FP64, 1 FP32, 2 16-bit)")
     a = ap.parse_args()
     from . import fields as F
     from . import stag as S
@@ -56,6 +59,23 @@ def main():
     g = F.naive_links(dims) if a.naive else F.fat_naik_links(dims)
     s = S.Staggered(S.Layout(dims), S.to_device_links(g))
     del g
+    if a.solve >= 0:
+        import time
+
+        import torch
+        b = S.to_device_vector(F.even_source(dims))
+        y = torch.zeros_like(b)
+        out = {}
+        for rep in ("warm", "timed"):
+            sp = S.SolverParams(r2req=1e-20, sloppySolve=a.solve)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.solveEE(y, b, 0.01, sp)
+            torch.cuda.synchronize()
+            out[rep] = {"seconds": time.perf_counter() - t0, "iterations": sp.iterations,
+                        "launches": sp.kernel_launches, "reliable_updates": sp.reliable_updates}
+        print(json.dumps({"dims": dims, "solve": a.solve, **out}))
+        return
     res = time_schur(s, F.volume(dims) // 2, [int(v) for v in a.prec.split(",")], a.nrep)
     print(json.dumps({"dims": dims, "nlinks": s.nlinks, "recon12": s.recon12, "schur": res}))
 
