@@ -17,9 +17,17 @@ constexpr int kF16 = 1;  // 16-bit fixed point (see h2f)
 // the largest magnitude maps to 32767.  This keeps 15 bits of resolution
 // relative to the largest element, where an IEEE half keeps 11.
 constexpr float kI16 = 32767.f;
-// raw integers of a packed pair, as floats (no scaling)
-__device__ __forceinline__ float2 h2f(unsigned u) {
-  return make_float2((float)(short)(u & 0xffffu), (float)(short)(u >> 16));
+// raw integers of a packed pair, as floats (no scaling).  An int->float
+// conversion instruction runs on the quarter-rate XU pipe and would bound
+// the 16-bit Dslash; instead flip the sign bits (two's complement -> offset
+// binary, u = i + 32768), place u in the mantissa of 2^23 and subtract
+// 2^23 + 32768: one logic op and one FP32 add per value, both full rate,
+// and exact for every 16-bit integer.
+__device__ __forceinline__ float2 h2f(unsigned w) {
+  const unsigned x = w ^ 0x80008000u;
+  const float lo = __uint_as_float(0x4B000000u | (x & 0xffffu)) - 8421376.0f;
+  const float hi = __uint_as_float(0x4B000000u | (x >> 16)) - 8421376.0f;
+  return make_float2(lo, hi);
 }
 // pack two values in [-1, 1]
 __device__ __forceinline__ unsigned f2h(float a, float b) {
