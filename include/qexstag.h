@@ -160,6 +160,18 @@ int qexstag_Ddag(qexstag_links *g, double *r, const double *x, double m, int mem
    r_p = 4 m2 x_p - (2D)_pq (2D)_qp x_p.  Full-lattice fields. */
 int qexstag_stagD2ee(qexstag_links *g, double *r, const double *x, double m2, int mem);
 int qexstag_stagD2oo(qexstag_links *g, double *r, const double *x, double m2, int mem);
+/* stagD2ee for device fields that allocates nothing; it has no counterpart in
+   QEX.  For callers that cannot let a library call cudaMalloc: hosts whose
+   own pool allocator already holds nearly all device memory, and hosts that
+   cannot accept the device-wide synchronisation of cudaMalloc/cudaFree in
+   the middle of an asynchronous pipeline.  r and x are device fields
+   (double2[3][V]); the result equals qexstag_stagD2ee(..., MEM_DEVICE).  The
+   odd-parity temporary is a static 3 MiB device array, so V/2 must be at most
+   65536 (larger lattices return QEXSTAG_ERR_ARG); every GPU that loads the
+   library holds it until exit.  All calls on a device share that array:
+   calls that overlap on the GPU race.  The first call on a device looks up
+   the array's address; make it before any stream capture. */
+int qexstag_stagD2ee_noalloc(qexstag_links *g, double *r, const double *x, double m2);
 
 /* ---- solvers (src/physics/stagSolve.nim, src/solvers/cg.nim, cgm.nim) ---- */
 

@@ -77,6 +77,7 @@ SIGNATURES = {
     "qexstag_Ddag": (I, [P, P, P, D, I]),
     "qexstag_stagD2ee": (I, [P, P, P, D, I]),
     "qexstag_stagD2oo": (I, [P, P, P, D, I]),
+    "qexstag_stagD2ee_noalloc": (I, [P, P, P, D]),
     "qexstag_solveEE": (I, [P, P, P, D, P, P, I]),
     "qexstag_solveOO": (I, [P, P, P, D, P, P, I]),
     "qexstag_solve": (I, [P, P, P, D, P, P, I]),

@@ -14,6 +14,8 @@
 //
 // Compulsory HBM bytes per output site: 8 (naive) or 16 (fat+Naik) links of
 // 144 B, plus 48 B in, 48 B out, plus 48 B per same-site init operand.
+#include <cstring>
+
 #include "lib.cuh"
 
 namespace qs {
@@ -206,6 +208,48 @@ int schur64(const qexstag_links_s *gl, int par, VecD r, CVecD x, VecD t, double 
   if (rc) return rc;
   return dslash64(gl, par, r, cv(t), x, CVecD{nullptr, 0}, 0.0, 4.0 * m2, 1.0, -1, 1, red, state,
                   done, dot_out);
+}
+
+}  // namespace qs
+
+namespace qs {
+
+// The FP64 Schur operator with a caller-provided temporary t, launched
+// without touching the library's reduction scratch (no reductions, no
+// early exit); used by the allocation-free entry point.
+int schur64_plain(const qexstag_links_s *gl, int par, VecD r, CVecD x, VecD t, double m2) {
+  const Geom &g = gl->l->g;
+  DslashArgs64 A;
+  std::memset(&A, 0, sizeof(A));
+  A.g = g;
+  A.u = gl->u64;
+  const int grid = grid_for(g.nh, kBlock, 6);
+  // t = (2D)_{q,par} x
+  A.po = 1 - par;
+  A.xin = x.p;
+  A.istride = x.stride;
+  A.out = t.p;
+  A.ostride = t.stride;
+  A.c = 1.0;
+  if (gl->nl == 8)
+    launch64<8, 1, 0, kRedNone>(A, grid);
+  else
+    launch64<4, 1, 0, kRedNone>(A, grid);
+  // r = 4 m2 x - (2D)_{par,q} t
+  A.po = par;
+  A.xin = t.p;
+  A.istride = t.stride;
+  A.xs = x.p;
+  A.sstride = x.stride;
+  A.out = r.p;
+  A.ostride = r.stride;
+  A.b = 4.0 * m2;
+  if (gl->nl == 8)
+    launch64<8, -1, 1, kRedNone>(A, grid);
+  else
+    launch64<4, -1, 1, kRedNone>(A, grid);
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
 }
 
 }  // namespace qs
