@@ -26,18 +26,42 @@ struct Geom {
   int stride[4];  // lexicographic strides: 1, L0, L0*L1, L0*L1*L2
   int V;
   int nh;  // sites per parity (V/2; all L are even)
+  // n / L[d] = umulhi(n, mag[d]) >> shf[d] for 0 <= n < 2^31 (d = 0, 1, 2):
+  // shf = floor(log2 L) and mag = ceil(2^(32+shf) / L), or mag = 2^31 and
+  // shf = log2(L) - 1 when L is a power of two (set by set_fastdiv)
+  unsigned mag[3];
+  int shf[3];
 };
+
+inline void set_fastdiv(Geom &g) {
+  for (int d = 0; d < 3; d++) {
+    const unsigned L = (unsigned)g.L[d];
+    int s = 0;
+    while ((2u << s) <= L) s++;  // floor(log2 L)
+    if ((L & (L - 1)) == 0) {
+      g.mag[d] = 1u << 31;
+      g.shf[d] = s - 1;
+    } else {
+      g.mag[d] = (unsigned)((((unsigned long long)1 << (32 + s)) + L - 1) / L);
+      g.shf[d] = s;
+    }
+  }
+}
+
+__device__ __forceinline__ int fdiv(const Geom &g, int d, int n) {
+  return (int)(__umulhi((unsigned)n, g.mag[d]) >> g.shf[d]);
+}
 
 // Coordinates and lex index of the k-th site of parity par.  Follows
 // qlayout.nim:108-136 with innerGeom = 1: idx = (lex + par*V)/2, so the
 // parity-par site k has lex 2k or 2k+1, whichever has parity par (L0 even).
 __device__ __forceinline__ void site_coords(const Geom &g, int par, int k, int x[4], int &lex) {
   int l0 = 2 * k;
-  int t = l0 / g.L[0];
+  int t = fdiv(g, 0, l0);
   int x0 = l0 - t * g.L[0];
-  int t2 = t / g.L[1];
+  int t2 = fdiv(g, 1, t);
   x[1] = t - t2 * g.L[1];
-  int t3 = t2 / g.L[2];
+  int t3 = fdiv(g, 2, t2);
   x[2] = t2 - t3 * g.L[2];
   x[3] = t3;
   int p0 = (x[1] + x[2] + x[3]) & 1;  // parity of lex l0 (x0 even)

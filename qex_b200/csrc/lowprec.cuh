@@ -12,28 +12,27 @@ namespace qs {
 constexpr int kF32 = 0;
 constexpr int kF16 = 1;  // 16-bit fixed point (see h2f)
 
-// 16-bit storage is fixed point: a signed 16-bit integer per real, scaled
-// by a per-site norm (colour vectors) or a per-list scale (links) so that
-// the largest magnitude maps to 32767.  This keeps 15 bits of resolution
-// relative to the largest element, where an IEEE half keeps 11.
+// 16-bit storage is fixed point: a 16-bit integer per real, scaled by a
+// per-site norm (colour vectors) or a per-list scale (links) so that the
+// largest magnitude maps to 32767.  This keeps 15 bits of resolution
+// relative to the largest element, where an IEEE half keeps 11.  The integer
+// i in [-32767, 32767] is stored in offset binary, u = i + 32768, so that a
+// load needs no int->float conversion instruction (those run on the
+// quarter-rate XU pipe and bounded the Dslash): one byte permute places u in
+// the low mantissa bits of 2^23 and one FP32 add subtracts 2^23 + 32768,
+// exactly, on full-rate pipes.
 constexpr float kI16 = 32767.f;
-// raw integers of a packed pair, as floats (no scaling).  An int->float
-// conversion instruction runs on the quarter-rate XU pipe and would bound
-// the 16-bit Dslash; instead flip the sign bits (two's complement -> offset
-// binary, u = i + 32768), place u in the mantissa of 2^23 and subtract
-// 2^23 + 32768: one logic op and one FP32 add per value, both full rate,
-// and exact for every 16-bit integer.
+// raw integers of a packed pair, as floats (no scaling)
 __device__ __forceinline__ float2 h2f(unsigned w) {
-  const unsigned x = w ^ 0x80008000u;
-  const float lo = __uint_as_float(0x4B000000u | (x & 0xffffu)) - 8421376.0f;
-  const float hi = __uint_as_float(0x4B000000u | (x >> 16)) - 8421376.0f;
+  const float lo = __uint_as_float(__byte_perm(w, 0x4B00u, 0x5410)) - 8421376.0f;
+  const float hi = __uint_as_float(__byte_perm(w, 0x4B00u, 0x5432)) - 8421376.0f;
   return make_float2(lo, hi);
 }
 // pack two values in [-1, 1]
 __device__ __forceinline__ unsigned f2h(float a, float b) {
-  int ia = __float2int_rn(fminf(fmaxf(a, -1.f), 1.f) * kI16);
-  int ib = __float2int_rn(fminf(fmaxf(b, -1.f), 1.f) * kI16);
-  return ((unsigned)ia & 0xffffu) | (((unsigned)ib & 0xffffu) << 16);
+  int ia = __float2int_rn(fminf(fmaxf(a, -1.f), 1.f) * kI16) + 32768;
+  int ib = __float2int_rn(fminf(fmaxf(b, -1.f), 1.f) * kI16) + 32768;
+  return ((unsigned)ia & 0xffffu) | ((unsigned)ib << 16);
 }
 
 // Link pointers of one handle as the kernels see them.

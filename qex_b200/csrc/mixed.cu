@@ -274,6 +274,13 @@ __device__ __forceinline__ bool mx_halt(const MxState *st) { return st->done || 
 // are kept apart so that the FP16 list scales multiply them once per site.
 // ---------------------------------------------------------------------------
 
+// Resident blocks per SM asked of ptxas: the 16-bit kernel is instruction-
+// heavy for the bytes it moves and gains from occupancy (4 blocks: 64
+// registers, 4450 GB/s on 32^4 against 4090 GB/s with 72-80 registers, same
+// grid); the FP32 kernel runs at the copy bandwidth with its natural 72
+// registers.  (Splitting a site's forward and backward hops over two threads
+// was slower: 3640-3720 GB/s.)
+
 struct DslashArgsLo {
   Geom g;
   int po;
@@ -293,7 +300,7 @@ struct DslashArgsLo {
 };
 
 template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
-__global__ void __launch_bounds__(kBlock) dslash_lo_kernel(const DslashArgsLo A) {
+__global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel(const DslashArgsLo A) {
   if (A.halt != nullptr && mx_halt(A.halt)) return;
   const Geom &g = A.g;
   const int nh = g.nh;
@@ -397,12 +404,39 @@ __global__ void __launch_bounds__(kBlock) dslash_lo_kernel(const DslashArgsLo A)
   }
 }
 
+// Grid of a sloppy half sweep.  The 16-bit kernel runs exactly two waves of
+// resident blocks (occupancy from the runtime, so that no partial wave idles
+// SMs: on 32^4 two waves gave 5208 GB/s, 1.5 waves 4437); the FP32 kernel is
+// at the copy bandwidth with 4 blocks per SM.
+template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
+static int lo_grid(int nh) {
+  static int resident = 0;  // one per kernel instantiation
+  if (resident == 0) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, R12>,
+                                                      kBlock, 0) != cudaSuccess ||
+        n < 1) {
+      cudaGetLastError();
+      n = 4;
+    }
+    resident = n;
+  }
+  long want = (long)num_sms() * (PREC == kF16 ? 2 * resident : 4);
+  long need = (nh + kBlock - 1) / kBlock;
+  long g = want < need ? want : need;
+  if (g > kMaxRedBlocks) g = kMaxRedBlocks;
+  return (int)(g < 1 ? 1 : g);
+}
+
 template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP>
-static void launch_lo(const DslashArgsLo &A, int grid) {
-  if (NL == 8 && A.L.recon12)
-    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 1><<<grid, kBlock, 0, stream()>>>(A);
-  else
-    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 0><<<grid, kBlock, 0, stream()>>>(A);
+static void launch_lo(const DslashArgsLo &A, int) {
+  if (NL == 8 && A.L.recon12) {
+    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 1>
+        <<<lo_grid<PREC, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, 0, stream()>>>(A);
+  } else {
+    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 0>
+        <<<lo_grid<PREC, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, 0, stream()>>>(A);
+  }
   note_launch();
 }
 
@@ -437,8 +471,7 @@ int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void
   A.partials = red_partials();
   A.ticket = red_tickets();
   A.dot_out = dot_out;
-  int grid = grid_for(geo.nh, kBlock, 6);
-  if (grid > kMaxRedBlocks) grid = kMaxRedBlocks;
+  const int grid = 0;  // chosen per kernel by launch_lo
   // half sweep 1
   A.po = 1 - par;
   A.xin = p;
