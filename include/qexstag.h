@@ -140,6 +140,11 @@ int qexstag_layout_shift_table(const qexstag_layout *l, int mu, int len, int sub
 int qexstag_links_create(qexstag_layout *l, int nlinks, const double *links, int mem,
                          double long_coeff, qexstag_links **out);
 int qexstag_links_destroy(qexstag_links *g);
+/* Replace the link data of a handle (same layout and nlinks) and rebuild its
+   reduced-precision copies.  QEX's Staggered.g references the gauge fields,
+   so an HMC update of U is seen by the next solve; with device copies the
+   caller calls this after changing the links. */
+int qexstag_links_update(qexstag_links *g, const double *links, int mem);
 /* 1 when the handle uses 12-real long links in its reduced precisions. */
 int qexstag_links_recon12(const qexstag_links *g);
 
@@ -217,6 +222,16 @@ int qexstag_force(qexstag_links *g, double *f, const double *phi, double m,
                   const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
 /* fermForce alone for a given psi (full lattice). */
 int qexstag_ferm_force(qexstag_links *g, double *f, const double *psi, int mem);
+/* stagForceSolve (hmcAction.nim:669-721) alone: psi = (4y, (2D)_oe 4y) with
+   stagD2ee(m^2) y = phi_e (full-lattice psi; the solve honours p->sloppy). */
+int qexstag_force_solve(qexstag_links *g, double *psi, const double *phi, double m,
+                        const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
+/* fermForce's outer products before the smearing chain rule and projection
+   (hmcAction.nim:744-771): f_k(x) = s(x) psi(x) psi(x + d_k)^dagger, s = +1 on
+   even and -1 on odd sites; for a fat+Naik list the long-link entries are
+   QEX's f3.  These are what a smearing derivative (QEX's u.deriv(ff, f1, f3))
+   consumes.  Layout as qexstag_force's f. */
+int qexstag_ferm_outer(qexstag_links *g, double *f, const double *psi, int mem);
 
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */

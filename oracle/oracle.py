@@ -62,6 +62,7 @@ def lib():
             "or_project_tah": (None, [P, P]),
             "or_force_solve": (I, [P, P, P, D, D, I, DP]),
             "or_ferm_force": (None, [P, P, P]),
+            "or_ferm_outer": (None, [P, P, P]),
             "or_force": (I, [P, P, P, D, D, I, DP]),
             "or_num_threads": (I, []),
         }
@@ -185,6 +186,9 @@ class Oracle:
 
     def ferm_force(self, f, psi):
         lib().or_ferm_force(self.ctx, _p(f), _p(psi))
+
+    def ferm_outer(self, f, psi):
+        lib().or_ferm_outer(self.ctx, _p(f), _p(psi))
 
     def force(self, f, phi, m, r2req, maxits=100000):
         r2 = C.c_double()

@@ -766,6 +766,28 @@ void or_ferm_force(void *ctx, double *f, const double *psi) {
   }
 }
 
+/* fermForce's outer products alone (hmcAction.nim:744-771): for link k,
+   f_k(x)[a,b] = s(x) psi_a(x) conj(psi_b(x + len mu)), s = -1 on odd x. */
+void or_ferm_outer(void *ctx, double *f, const double *psi) {
+  OCtx *c = (OCtx *)ctx;
+  const long V = c->V;
+  for (int k = 0; k < c->nlinks; k++) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < V; i++) {
+      const double *a = psi + 6 * i;
+      const double *bb = psi + 6 * (long)c->fwd[k * V + i];
+      double s = (i >= c->nEven) ? -1.0 : 1.0;
+      double *o = f + ((long)k * V + i) * 18;
+      for (int p = 0; p < 3; p++)
+        for (int q = 0; q < 3; q++) {
+          double ar = a[2 * p], ai = a[2 * p + 1], br = bb[2 * q], bi = -bb[2 * q + 1];
+          o[6 * p + 2 * q] = s * (ar * br - ai * bi);
+          o[6 * p + 2 * q + 1] = s * (ar * bi + ai * br);
+        }
+    }
+  }
+}
+
 /* stagForceSolve followed by fermForce: the force QEX's
    StaggeredFermionAction.force hands to addForce (before its 0.25*dtau). */
 int or_force(void *ctx, double *f, const double *phi, double m, double r2req, int maxits,

@@ -71,6 +71,7 @@ SIGNATURES = {
     "qexstag_links_create": (I, [P, I, P, I, D, C.POINTER(P)]),
     "qexstag_links_destroy": (I, [P]),
     "qexstag_links_recon12": (I, [P]),
+    "qexstag_links_update": (I, [P, P, I]),
     "qexstag_stagD2": (I, [P, I, P, P, D, D, I]),
     "qexstag_stagD": (I, [P, I, P, P, D, D, D, I]),
     "qexstag_D": (I, [P, P, P, D, I]),
@@ -85,6 +86,8 @@ SIGNATURES = {
     "qexstag_cgm_ee": (I, [P, D, I, DP, I, PP, PP, P, P, DP, I]),
     "qexstag_force": (I, [P, P, P, D, P, P, I]),
     "qexstag_ferm_force": (I, [P, P, P, I]),
+    "qexstag_force_solve": (I, [P, P, P, D, P, P, I]),
+    "qexstag_ferm_outer": (I, [P, P, P, I]),
     "qexstag_bench_schur": (I, [P, I, I, D, DP]),
 }
 

@@ -160,6 +160,7 @@ static void init_stats(qexstag_solver_stats *st) {
   st->kernel_launches = -launch_count();  // completed by finish_stats
 }
 static void finish_stats(qexstag_solver_stats *st) { st->kernel_launches += launch_count(); }
+static double geo_nh(const qexstag_links_s *g) { return (double)g->l->g.nh; }
 
 }  // namespace qs
 
@@ -257,6 +258,30 @@ int qexstag_layout_shift_table(const qexstag_layout *l, int mu, int len, int sub
 // links
 // ---------------------------------------------------------------------------
 
+}  // extern "C"
+
+namespace qs {
+// copy a link list into g->u64 (host AoS layout or device SoA layout)
+static int upload_links(qexstag_links_s *g, const double *links, int mem) {
+  const Geom &geo = g->l->g;
+  const size_t per = sizeof(double2) * 9 * (size_t)geo.V;
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    QS_CUDA(cudaMemcpyAsync(g->u64, links, per * g->nl, cudaMemcpyDeviceToDevice, stream()));
+    return QEXSTAG_OK;
+  }
+  void *aos;
+  int rc = g->ws.get(kSlotAos, per, &aos);
+  if (rc) return rc;
+  for (int k = 0; k < g->nl; k++) {
+    QS_CUDA(cudaMemcpyAsync(aos, links + (size_t)k * 18 * geo.V, per, cudaMemcpyHostToDevice, stream()));
+    if ((rc = aos_to_soa((const double *)aos, g->u64 + (size_t)k * 9 * geo.V, geo.V, geo.V, 9))) return rc;
+  }
+  return QEXSTAG_OK;
+}
+}  // namespace qs
+
+extern "C" {
+
 int qexstag_links_create(qexstag_layout *l, int nlinks, const double *links, int mem,
                          double long_coeff, qexstag_links **out) {
   if (!l || !links || !out) return fail(QEXSTAG_ERR_ARG, "links_create: null argument");
@@ -278,31 +303,11 @@ int qexstag_links_create(qexstag_layout *l, int nlinks, const double *links, int
     delete g;
     return fail(QEXSTAG_ERR_ALLOC, "links_create: device allocation failed");
   }
-  if (mem == QEXSTAG_MEM_DEVICE) {
-    e = cudaMemcpyAsync(g->u64, links, per * nlinks, cudaMemcpyDeviceToDevice, stream());
-    if (e != cudaSuccess) {
-      cudaFree(g->u64);
-      delete g;
-      return cuda_fail(e, "links_create copy");
-    }
-  } else {
-    void *aos;
-    if ((rc = g->ws.get(kSlotAos, per, &aos))) {
-      cudaFree(g->u64);
-      delete g;
-      return rc;
-    }
-    for (int k = 0; k < nlinks; k++) {
-      e = cudaMemcpyAsync(aos, links + (size_t)k * 18 * geo.V, per, cudaMemcpyHostToDevice, stream());
-      if (e != cudaSuccess) break;
-      if ((rc = aos_to_soa((const double *)aos, g->u64 + (size_t)k * 9 * geo.V, geo.V, geo.V, 9))) break;
-    }
-    if (e != cudaSuccess || rc) {
-      g->ws.release();
-      cudaFree(g->u64);
-      delete g;
-      return e != cudaSuccess ? cuda_fail(e, "links_create upload") : rc;
-    }
+  if ((rc = upload_links(g, links, mem))) {
+    g->ws.release();
+    cudaFree(g->u64);
+    delete g;
+    return rc;
   }
   if ((rc = build_low_links(g))) {
     g->ws.release();
@@ -314,6 +319,17 @@ int qexstag_links_create(qexstag_layout *l, int nlinks, const double *links, int
   e = cudaStreamSynchronize(stream());
   if (e != cudaSuccess) return cuda_fail(e, "links_create");
   *out = g;
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_update(qexstag_links *g, const double *links, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (!links) return fail(QEXSTAG_ERR_ARG, "links_update: null links");
+  if ((rc = upload_links(g, links, mem))) return rc;
+  free_low_links(g->low);
+  if ((rc = build_low_links(g))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
 }
 
@@ -602,6 +618,59 @@ int qexstag_ferm_force(qexstag_links *g, double *f, const double *psi, int mem) 
   return force_out(g, df, f, mem);
 }
 
+int qexstag_ferm_outer(qexstag_links *g, double *f, const double *psi, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (!f || !psi) return fail(QEXSTAG_ERR_ARG, "ferm_outer: null field");
+  const double2 *dpsi;
+  double2 *df;
+  if ((rc = stage_in(g, kSlotIn0, psi, mem, &dpsi))) return rc;
+  if ((rc = force_buf(g, f, mem, &df))) return rc;
+  if ((rc = ferm_outer64(g, df, dpsi))) return rc;
+  return force_out(g, df, f, mem);
+}
+
+// stagForceSolve (hmcAction.nim:669-721) into a full-lattice psi
+static int force_solve_dev(qexstag_links *g, double2 *psi, const double2 *phi, double m,
+                           const qexstag_solver_params *p, qexstag_solver_stats *st) {
+  const Geom &geo = g->l->g;
+  void *pvar;
+  int rc;
+  if ((rc = g->ws.get(kSlotFull1, sizeof(double2) * 3 * (size_t)geo.V, &pvar))) return rc;
+  double2 *varphi = (double2 *)pvar;
+  int status = solve_xx(g, 0, varphi, phi, m, p, st);
+  if (status < 0) return status;
+  if ((rc = vscale(block(varphi, geo, 0), 4.0, geo.nh))) return rc;
+  // psi_o = (2D)_oe varphi_e (stagD2 with a = b = 0); psi_e = varphi_e
+  if ((rc = dslash64(g, 1, block(psi, geo, 1), block((const double2 *)varphi, geo, 0), CVecD{nullptr, 0},
+                     CVecD{nullptr, 0}, 0.0, 0.0, 1.0, +1, 0)))
+    return rc;
+  if ((rc = vcopy(block(psi, geo, 0), block((const double2 *)varphi, geo, 0), geo.nh))) return rc;
+  return status;
+}
+
+int qexstag_force_solve(qexstag_links *g, double *psi, const double *phi, double m,
+                        const qexstag_solver_params *p, qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (!psi || !phi) return fail(QEXSTAG_ERR_ARG, "force_solve: null field");
+  qexstag_solver_stats st;
+  init_stats(&st);
+  Timer tm;
+  const double2 *dphi;
+  double2 *dpsi;
+  if ((rc = stage_in(g, kSlotIn0, phi, mem, &dphi))) return rc;
+  if ((rc = stage_out_buf(g, kSlotOut0, psi, mem, &dpsi))) return rc;
+  int status = force_solve_dev(g, dpsi, dphi, m, p, &st);
+  if (status < 0) return status;
+  if ((rc = stage_out_finish(g, dpsi, psi, mem))) return rc;
+  st.seconds = tm.seconds();
+  st.flops = (double)(g->nl * 4 * 72 + 60) * geo_nh(g) * st.iterations;
+  finish_stats(&st);
+  if (st_out) *st_out = st;
+  return status;
+}
+
 int qexstag_force(qexstag_links *g, double *f, const double *phi, double m,
                   const qexstag_solver_params *p, qexstag_solver_stats *st_out, int mem) {
   int rc;
@@ -613,21 +682,14 @@ int qexstag_force(qexstag_links *g, double *f, const double *phi, double m,
   Timer tm;
   const double2 *dphi;
   double2 *df;
-  void *pvar, *ppsi;
+  void *ppsi;
   const size_t fb = sizeof(double2) * 3 * (size_t)geo.V;
   if ((rc = stage_in(g, kSlotIn0, phi, mem, &dphi))) return rc;
   if ((rc = force_buf(g, f, mem, &df))) return rc;
-  if ((rc = g->ws.get(kSlotFull1, fb, &pvar)) || (rc = g->ws.get(kSlotIn1, fb, &ppsi))) return rc;
-  double2 *varphi = (double2 *)pvar, *psi = (double2 *)ppsi;
-  // stagForceSolve (hmcAction.nim:669-721)
-  int status = solve_xx(g, 0, varphi, dphi, m, p, &st);
+  if ((rc = g->ws.get(kSlotIn1, fb, &ppsi))) return rc;
+  double2 *psi = (double2 *)ppsi;
+  int status = force_solve_dev(g, psi, dphi, m, p, &st);
   if (status < 0) return status;
-  if ((rc = vscale(block(varphi, geo, 0), 4.0, geo.nh))) return rc;
-  // psi_o = (2D)_oe varphi_e (stagD2 with a = b = 0); psi_e = varphi_e
-  if ((rc = dslash64(g, 1, block(psi, geo, 1), block((const double2 *)varphi, geo, 0),
-                     CVecD{nullptr, 0}, CVecD{nullptr, 0}, 0.0, 0.0, 1.0, +1, 0)))
-    return rc;
-  if ((rc = vcopy(block(psi, geo, 0), block((const double2 *)varphi, geo, 0), geo.nh))) return rc;
   if ((rc = ferm_force64(g, df, psi))) return rc;
   if ((rc = force_out(g, df, f, mem))) return rc;
   st.seconds = tm.seconds();

@@ -71,6 +71,53 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
+// fermForce's outer products alone (hmcAction.nim:744-771), before the
+// smearing chain rule and the projection: f_k(x) = s(x) psi(x) psi(x+d_k)^dagger
+template <int NL>
+__global__ void __launch_bounds__(kBlock)
+    ferm_outer_kernel(Geom g, const double2 *__restrict__ psi, double2 *__restrict__ f) {
+  const size_t V = (size_t)g.V;
+  const int total = g.V * NL;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int l = t / g.V;
+    const int site = t - l * g.V;
+    const int par = site >= g.nh ? 1 : 0;
+    int x[4], lex;
+    site_coords(g, par, site - par * g.nh, x, lex);
+    const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
+    const size_t nb = (size_t)(1 - par) * g.nh + nbr_half(g, x, lex, mu, len);
+    double2 a[3], b[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      a[c] = ldg(psi + (size_t)c * V + site);
+      b[c] = ldg(psi + (size_t)c * V + nb);
+    }
+    const double s = par ? -1.0 : 1.0;
+    double2 *fl = f + (size_t)l * 9 * V + site;
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const double2 ap = a[p], bq = b[q];
+        // s * a_p * conj(b_q)
+        __stcs(fl + (size_t)(3 * p + q) * V,
+               make_double2(s * (ap.x * bq.x + ap.y * bq.y), s * (ap.y * bq.x - ap.x * bq.y)));
+      }
+  }
+}
+
+int ferm_outer64(qexstag_links_s *g, double2 *f, const double2 *psi) {
+  const Geom &geo = g->l->g;
+  const int grid = grid_for((long)geo.V * g->nl, kBlock, 8);
+  if (g->nl == 8)
+    ferm_outer_kernel<8><<<grid, kBlock, 0, stream()>>>(geo, psi, f);
+  else
+    ferm_outer_kernel<4><<<grid, kBlock, 0, stream()>>>(geo, psi, f);
+  note_launch();
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
 int ferm_force64(qexstag_links_s *g, double2 *f, const double2 *psi) {
   const Geom &geo = g->l->g;
   const long total = (long)geo.V * g->nl;

@@ -117,5 +117,6 @@ int solve_full(qexstag_links_s *g, double2 *x, const double2 *b, double m,
 
 // ---- force.cu ----
 int ferm_force64(qexstag_links_s *g, double2 *f, const double2 *psi);
+int ferm_outer64(qexstag_links_s *g, double2 *f, const double2 *psi);
 
 }  // namespace qs

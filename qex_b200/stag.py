@@ -178,6 +178,11 @@ class Staggered:
         self.handle = h
         self.nlinks = nl
 
+    def update_links(self, links) -> None:
+        """New link data for this operator (QEX's Staggered.g changed)."""
+        ptr, mem = _ptr(links)
+        L.check(self._lib.qexstag_links_update(self.handle, ptr, mem), "links_update")
+
     @property
     def recon12(self) -> bool:
         return bool(self._lib.qexstag_links_recon12(self.handle))
@@ -292,6 +297,17 @@ class Staggered:
                                      C.byref(p), C.byref(st), mem)
         L.check(rc, "force")
         sp.take(st, rc)
+
+    def force_solve(self, psi, phi, m: float, sp: SolverParams) -> None:
+        """stagForceSolve: psi = (4y, (2D)_oe 4y), stagD2ee(m^2) y = phi_e."""
+        self._solve_call(self._lib.qexstag_force_solve, "force_solve", psi, phi, m, sp)
+
+    def ferm_outer(self, f, psi) -> None:
+        """fermForce's outer products f1 (and f3 for long links), odd sites
+        negated, before the chain rule and projection."""
+        mem = _mem_of(f, psi)
+        L.check(self._lib.qexstag_ferm_outer(self.handle, _ptr(f, True)[0], _ptr(psi)[0], mem),
+                "ferm_outer")
 
     def ferm_force(self, f, psi) -> None:
         mem = _mem_of(f, psi)
