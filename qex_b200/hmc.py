@@ -280,9 +280,26 @@ def trajectory_with_reversal(lat, U0, beta, mass, naik, tau, nsteps, seed=7, slo
             "solver_iterations": ferm.solver_iterations}
 
 
+def thermalize(lat, U, beta, ntraj, tau=1.0, nsteps=20, seed=11):
+    """Pure-gauge HMC trajectories with Metropolis accept/reject
+    (src/hmc/metropolis.nim) to bring a warm start near equilibrium."""
+    rng = np.random.default_rng(seed)
+    hmc = HMC(lat, beta, None)
+    acc = 0
+    for _ in range(ntraj):
+        p = random_momenta(lat, rng)
+        h0 = hmc.hamiltonian(U, p)
+        U1, p1 = hmc.leapfrog(U, p, tau, nsteps)
+        dh = hmc.hamiltonian(U1, p1) - h0
+        if dh <= 0 or rng.random() < np.exp(-dh):
+            U, acc = U1, acc + 1
+    return U, acc
+
+
 def main():
     """Config 4: 16^4, beta 5.6, one pseudofermion (m = 0.05), tau = 1,
-    20 leapfrog steps, reversibility check."""
+    20 leapfrog steps, reversibility check (after --therm pure-gauge
+    thermalisation trajectories from a warm start)."""
     import argparse
     import json
     ap = argparse.ArgumentParser()
@@ -292,6 +309,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--tau", type=float, default=1.0)
     ap.add_argument("--naive", action="store_true")
+    ap.add_argument("--therm", type=int, default=10)
     a = ap.parse_args()
     dims = tuple(int(v) for v in a.dims.split(","))
     S.init(0)
@@ -299,8 +317,12 @@ def main():
     U0 = torch.from_numpy(F.gauge_warm(dims, 0.3, 41)).to("cuda")
     import time
     t0 = time.perf_counter()
+    U0, acc = thermalize(lat, U0, a.beta, a.therm)
+    t1 = time.perf_counter()
     out = trajectory_with_reversal(lat, U0, a.beta, a.mass, None if a.naive else -1.0 / 24.0, a.tau, a.steps)
-    out["seconds"] = time.perf_counter() - t0
+    out["seconds"] = time.perf_counter() - t1
+    out["thermalization"] = {"trajectories": a.therm, "accepted": acc, "seconds": t1 - t0}
+    out["plaquette"] = -out.pop("plaquette_action") / (a.beta / 3.0) / (6 * lat.V * 3)
     out["dims"] = dims
     print(json.dumps(out))
 
