@@ -210,6 +210,21 @@ int qexstag_cgm_ee(qexstag_links *g, double m, int nshift, const double *sigma, 
                    const qexstag_solver_params *p, qexstag_solver_stats *st,
                    double *r2_out, int mem);
 
+/* Many independent even-site solves in one persistent launch: for each
+   problem j (its own link handle, lattice and mass) solve
+   stagD2ee(mass[j]^2) x[j] = b[j] on even sites as solveEE does (FP64 CG,
+   cg.nim:55-272, then the FP64 true residual and defect correction,
+   stagSolve.nim:330-421).  All problems iterate together in one cooperative
+   kernel, captured in a CUDA graph; its block size and blocks per SM are
+   chosen by timing candidates on the first call for a problem set.
+   iterations[j] (and r2_out[j] = true |b - Ax|^2/|b|^2, optional) receive
+   the per-problem results; launch_info (optional, 3 ints) receives the
+   chosen block size, blocks per SM and 1 if the graph was used.  p->sloppy
+   must be NONE; at most 128 problems, each with its own handle. */
+int qexstag_solve_batched(int nprob, qexstag_links *const *g, const double *mass, double *const *x,
+                          const double *const *b, const qexstag_solver_params *p, int *iterations,
+                          double *r2_out, int *launch_info, qexstag_solver_stats *st, int mem);
+
 /* ---- HMC force (src/hmc/hmcAction.nim:669-790, 851-885) ---- */
 
 /* stagForceSolve followed by fermForce without smearing: solves

@@ -84,6 +84,7 @@ SIGNATURES = {
     "qexstag_solve": (I, [P, P, P, D, P, P, I]),
     "qexstag_solve_multishift": (I, [P, I, PP, P, DP, P, P, I]),
     "qexstag_cgm_ee": (I, [P, D, I, DP, I, PP, PP, P, P, DP, I]),
+    "qexstag_solve_batched": (I, [I, PP, DP, PP, PP, P, C.POINTER(C.c_int), DP, C.POINTER(C.c_int), P, I]),
     "qexstag_force": (I, [P, P, P, D, P, P, I]),
     "qexstag_ferm_force": (I, [P, P, P, I]),
     "qexstag_force_solve": (I, [P, P, P, D, P, P, I]),

@@ -576,6 +576,69 @@ int qexstag_cgm_ee(qexstag_links *g, double m, int nshift, const double *sigma, 
   return status;
 }
 
+}  // extern "C"
+
+namespace qs {
+int solve_batched(int nprob, qexstag_links_s *const *gs, const double *mass, double2 *const *x,
+                  const double2 *const *b, const qexstag_solver_params *p, int *iters, double *r2_out,
+                  qexstag_solver_stats *st, int *tuned_block, int *tuned_per_sm, int *graph_used);
+}
+
+extern "C" {
+
+int qexstag_solve_batched(int nprob, qexstag_links *const *g, const double *mass, double *const *x,
+                          const double *const *b, const qexstag_solver_params *p, int *iterations,
+                          double *r2_out, int *launch_info, qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_mem(mem)) || (rc = check_params(p))) return rc;
+  if (nprob < 1 || nprob > 128 || !g || !mass || !x || !b || !iterations)
+    return fail(QEXSTAG_ERR_ARG, "solve_batched: need 1..128 problems and non-null arrays");
+  if (p->sloppy != QEXSTAG_SLOPPY_NONE)
+    return fail(QEXSTAG_ERR_ARG, "solve_batched: the batched persistent solver is FP64 (sloppy NONE)");
+  for (int j = 0; j < nprob; j++) {
+    if ((rc = check_links(g[j]))) return rc;
+    if (g[j]->nl != g[0]->nl) return fail(QEXSTAG_ERR_ARG, "solve_batched: all problems need the same nlinks");
+    if (!x[j] || !b[j]) return fail(QEXSTAG_ERR_ARG, "solve_batched: null field");
+    for (int i = 0; i < j; i++)
+      if (g[i] == g[j]) return fail(QEXSTAG_ERR_ARG, "solve_batched: one link handle per problem");
+  }
+  qexstag_solver_stats st;
+  init_stats(&st);
+  Timer tm;
+  std::vector<const double2 *> db(nprob);
+  std::vector<double2 *> dx(nprob);
+  for (int j = 0; j < nprob; j++) {
+    if ((rc = stage_in(g[j], kSlotIn0, b[j], mem, &db[j]))) return rc;
+    if ((rc = stage_out_buf(g[j], kSlotOut0, x[j], mem, &dx[j]))) return rc;
+    const Geom &geo = g[j]->l->g;
+    if ((rc = vzero(VecD{dx[j] + geo.nh, geo.V}, geo.nh))) return rc;  // odd sites: 0 (solveEE)
+  }
+  std::vector<double2 *> xe(nprob);
+  std::vector<const double2 *> be(nprob);
+  for (int j = 0; j < nprob; j++) {
+    xe[j] = dx[j];
+    be[j] = db[j];
+  }
+  int blk = 0, per_sm = 0, graph = 0;
+  int status = solve_batched(nprob, g, mass, xe.data(), be.data(), p, iterations, r2_out, &st, &blk, &per_sm,
+                             &graph);
+  if (status < 0) return status;
+  for (int j = 0; j < nprob; j++)
+    if ((rc = stage_out_finish(g[j], dx[j], x[j], mem))) return rc;
+  st.seconds = tm.seconds();
+  double fl = 0;
+  for (int j = 0; j < nprob; j++) fl += (double)(g[j]->nl * 4 * 72 + 60) * g[j]->l->g.nh * iterations[j];
+  st.flops = fl;
+  finish_stats(&st);
+  if (launch_info) {
+    launch_info[0] = blk;
+    launch_info[1] = per_sm;
+    launch_info[2] = graph;
+  }
+  if (st_out) *st_out = st;
+  return status;
+}
+
 // ---------------------------------------------------------------------------
 // force
 // ---------------------------------------------------------------------------

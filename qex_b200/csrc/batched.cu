@@ -1,0 +1,729 @@
+// batched.cu -- many independent even-odd CG solves in one persistent
+// launch.
+//
+// Each problem j has its own lattice (own dims), links, mass and source and
+// solves stagD2ee(m_j^2) x_j = b_j on its even sites with QEX's CG
+// (src/solvers/cg.nim:174-240, cpNone).  Small lattices cannot fill a B200
+// alone and a per-problem solve is bound by kernel launches (four per
+// iteration); here every problem's sites are concatenated into one index
+// space, split into equal contiguous chunks, one per block of a cooperative
+// grid (rebuilt every iteration over the problems still iterating, so that
+// the last, slowest problems still use every SM), and the whole CG runs
+// inside one kernel:
+//   phase A  t_j = (2D)_oe p_j  with p_j = r_j + beta_j p_j formed at the
+//            neighbours on the fly (odd output sites)
+//   phase B  p_j = r_j + beta_j p_j; Ap_j = 4 m_j^2 p_j - (2D)_eo t_j;
+//            <p_j, Ap_j> -> alpha_j
+//   phase C  x_j += alpha_j p_j; r_j -= alpha_j Ap_j; |r_j|^2 -> beta_j, done_j
+// separated by grid barriers.  A problem's scalars come from per-site
+// contributions summed, in a fixed order, by the last block to finish that
+// problem (a per-problem ticket), so results are bitwise reproducible.
+// Finished problems drop out; the kernel returns when none is active.
+//
+// Every wait is bounded: a barrier that has not completed within the time
+// limit sets an error flag and all blocks return; the host reports
+// QEXSTAG_ERR_TIMEOUT.  Data written inside the kernel is read with L2-only
+// loads, because L1 is not coherent across SMs.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "lib.cuh"
+
+namespace qs {
+
+int cg64(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, int maxits, CgOut *out);
+
+constexpr int kMaxBatch = 128;
+
+struct BProb {
+  Geom g;
+  const double2 *u;  // [nl][9][V]
+  const double2 *b;  // even block of b (stride V)
+  double2 *x;        // even block of x (stride V)
+  double2 *r, *p, *ap, *t;  // [3][nh]
+  double m2;
+  int off;  // first index of this problem's entries in the per-site buffer
+  int pad;
+};
+
+struct BState {
+  double rz, r2, b2, r2stop, alpha, beta, pAp, r2req;
+  int itn, done, maxits, pad;
+  unsigned ticket, pad2;
+};
+
+struct BGlobal {
+  unsigned bar_count;
+  unsigned bar_gen;
+  int err;
+  int active;
+};
+
+struct BArgs {
+  const BProb *probs;
+  BState *st;
+  BGlobal *glob;
+  double *dot;   // one double per concatenated site
+  double *part;  // per-problem block partials, part_stride per problem
+  int part_stride;
+  int nprob;
+  int ntot;
+  long long timeout_cycles;
+};
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int ld_int(const int *p) { return *(volatile const int *)p; }
+__device__ __forceinline__ double ld_dbl(const double *p) { return __ldcg(p); }
+
+// Grid barrier with a time limit; returns false (in every thread) when the
+// barrier failed or another block reported an error.
+__device__ bool grid_sync(BGlobal *gl, long long timeout) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned gen = *(volatile unsigned *)&gl->bar_gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&gl->bar_count, 1u);
+    if (arrived == gridDim.x - 1) {
+      gl->bar_count = 0;
+      __threadfence();
+      atomicAdd(&gl->bar_gen, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*(volatile unsigned *)&gl->bar_gen == gen) {
+        if (ld_int(&gl->err)) break;
+        if (clock64() - t0 > timeout) {
+          atomicExch(&gl->err, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok = ld_int(&gl->err) == 0;
+  }
+  __syncthreads();
+  return ok;
+}
+
+__device__ __forceinline__ int find_prob(const int *offs, int n, int s) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (offs[mid] <= s)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ double2 ld2(const double2 *p) { return __ldcg(p); }
+
+// sum over k in [0,n) of dot[k] by one block, fixed order
+__device__ double block_sum_range(const double *dot, int n) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += ld_dbl(dot + i);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[w] = s;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)((blockDim.x + 31) >> 5); i++) t += sh[i];
+  return t;  // valid in thread 0
+}
+
+// The partition of one iteration: the still-active problems (ids, in
+// order) laid end to end, aoff[i] the first index of the i-th, cut into
+// equal contiguous chunks, one per block.  Every block builds the same table
+// after a grid barrier, so the work of the remaining problems is always
+// spread over the whole grid.
+struct Part {
+  int na;        // active problems
+  int ntot;      // their sites
+  int chunk;
+  int c0, c1;    // this block's range
+  int ids[kMaxBatch];
+  int aoff[kMaxBatch];
+};
+
+__device__ void build_part(const BArgs &A, const BProb *P, Part &T, bool all) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int n = 0, off = 0;
+    for (int j = 0; j < A.nprob; j++) {
+      if (!all && ld_int(&A.st[j].done)) continue;
+      T.ids[n] = j;
+      T.aoff[n] = off;
+      off += P[j].g.nh;
+      n++;
+    }
+    T.na = n;
+    T.ntot = off;
+    T.chunk = (off + gridDim.x - 1) / gridDim.x;
+    T.c0 = min(off, (int)blockIdx.x * T.chunk);
+    T.c1 = min(off, T.c0 + T.chunk);
+  }
+  __syncthreads();
+}
+
+// After a block has written its per-site contributions (A.dot indexed by the
+// problem's own offset P[j].off): for every problem its chunk meets, the
+// block sums its own part of the problem's entries and stores that partial
+// at the block's slot for the problem; the last block of a problem sums the
+// partials in slot order and runs fin(j, sum) in thread 0.  The order of
+// every sum is fixed by the partition, which is the same on every run.
+template <class Fin>
+__device__ void finish_chunk(const BArgs &A, const BProb *P, const Part &T, Fin fin) {
+  __shared__ int last;
+  if (T.c0 >= T.c1) return;
+  __syncthreads();  // the block's per-site entries are all written
+  const int i0 = find_prob(T.aoff, T.na, T.c0), i1 = find_prob(T.aoff, T.na, T.c1 - 1);
+  for (int i = i0; i <= i1; i++) {
+    const int j = T.ids[i];
+    const int lo = T.aoff[i], hi = lo + P[j].g.nh;
+    const int b0 = lo / T.chunk;
+    const unsigned nb = (unsigned)((hi - 1) / T.chunk - b0 + 1);
+    const int s0 = max(lo, T.c0), s1 = min(hi, T.c1);  // this block's part
+    const double part = block_sum_range(A.dot + P[j].off + (s0 - lo), s1 - s0);
+    if (threadIdx.x == 0) {
+      A.part[(size_t)j * A.part_stride + (blockIdx.x - b0)] = part;
+      __threadfence();
+      const unsigned t = atomicAdd(&A.st[j].ticket, 1u);
+      last = (t == nb - 1);
+    }
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      const double s = block_sum_range(A.part + (size_t)j * A.part_stride, (int)nb);
+      if (threadIdx.x == 0) {
+        A.st[j].ticket = 0;
+        fin(j, s);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// one staggered hop sum at output site k of parity po for problem P, with
+// the input vector at neighbour sites produced by load(j, c)
+template <int NL, int HOP, class Load>
+__device__ __forceinline__ void hop_sum(const BProb &P, int po, int k, Load load, double2 acc[3]) {
+  const Geom &g = P.g;
+  const size_t V = (size_t)g.V;
+  const size_t in_base = (size_t)(1 - po) * g.nh, out_base = (size_t)po * g.nh;
+  int x[4], lex;
+  site_coords(g, po, k, x, lex);
+#pragma unroll
+  for (int l = 0; l < NL; l++) {
+    const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
+    const int jf = nbr_half(g, x, lex, mu, len);
+    const int jb = nbr_half(g, x, lex, mu, -len);
+    const double2 *ul = P.u + (size_t)l * 9 * V;
+    double2 v[3], w[3], uf[9], ub[9];
+    load(jf, v);
+    load(jb, w);
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+      uf[e] = ldg(ul + (size_t)e * V + out_base + k);
+      ub[e] = ldg(ul + (size_t)e * V + in_base + jb);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      double2 t = make_double2(0.0, 0.0), q = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        t = cmadd(t, uf[3 * i + c], v[c]);
+        q = cjmadd(q, ub[3 * c + i], w[c]);
+      }
+      if (HOP > 0) {
+        acc[i].x += t.x - q.x;
+        acc[i].y += t.y - q.y;
+      } else {
+        acc[i].x -= t.x - q.x;
+        acc[i].y -= t.y - q.y;
+      }
+    }
+  }
+}
+
+template <int NL>
+__global__ void batched_cg_kernel(const BArgs A) {
+  __shared__ BProb P[kMaxBatch];
+  __shared__ Part T;
+  for (int j = threadIdx.x; j < A.nprob; j += blockDim.x) P[j] = A.probs[j];
+  const long long tmo = A.timeout_cycles;
+  build_part(A, P, T, true);
+
+  // ---- init: r = b, x = 0, p = 0; |b|^2 ----
+  for (int s = T.c0 + threadIdx.x; s < T.c1; s += blockDim.x) {
+    const int i = find_prob(T.aoff, T.na, s);
+    const BProb &Q = P[T.ids[i]];
+    const int k = s - T.aoff[i], V = Q.g.V, nh = Q.g.nh;
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 bv = ldg(Q.b + (size_t)c * V + k);
+      Q.r[(size_t)c * nh + k] = bv;
+      Q.p[(size_t)c * nh + k] = make_double2(0.0, 0.0);
+      Q.x[(size_t)c * V + k] = make_double2(0.0, 0.0);
+      acc = fma(bv.x, bv.x, acc);
+      acc = fma(bv.y, bv.y, acc);
+    }
+    A.dot[Q.off + k] = acc;
+  }
+  finish_chunk(A, P, T, [&](int j, double b2) {
+    BState &S = A.st[j];
+    S.b2 = b2;
+    S.rz = S.r2 = b2;
+    S.r2stop = S.r2req * b2;
+    S.itn = 0;
+    S.beta = 0.0;
+    const int d = (!(b2 > S.r2stop) || S.maxits <= 0 || isnan(b2)) ? 1 : 0;
+    S.done = d;
+    if (d) atomicSub(&A.glob->active, 1);
+  });
+  if (!grid_sync(A.glob, tmo)) return;
+
+  for (;;) {
+    if (ld_int(&A.glob->active) <= 0) break;
+    build_part(A, P, T, false);
+    // ---- phase A: t = (2D)_oe (r + beta p) on odd sites ----
+    for (int s = T.c0 + threadIdx.x; s < T.c1; s += blockDim.x) {
+      const int i = find_prob(T.aoff, T.na, s);
+      const int j = T.ids[i];
+      const BProb &Q = P[j];
+      const int k = s - T.aoff[i], nh = Q.g.nh;
+      const double beta = ld_dbl(&A.st[j].beta);
+      double2 acc[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+      hop_sum<NL, 1>(Q, 1, k, [&](int n, double2 v[3]) {
+        for (int c = 0; c < 3; c++) {
+          const double2 rv = ld2(Q.r + (size_t)c * nh + n), pv = ld2(Q.p + (size_t)c * nh + n);
+          v[c] = make_double2(fma(beta, pv.x, rv.x), fma(beta, pv.y, rv.y));
+        }
+      }, acc);
+#pragma unroll
+      for (int c = 0; c < 3; c++) Q.t[(size_t)c * nh + k] = acc[c];
+    }
+    if (!grid_sync(A.glob, tmo)) return;
+    // ---- phase B: p = r + beta p; Ap = 4 m2 p - (2D)_eo t; <p, Ap> ----
+    for (int s = T.c0 + threadIdx.x; s < T.c1; s += blockDim.x) {
+      const int i = find_prob(T.aoff, T.na, s);
+      const int j = T.ids[i];
+      const BProb &Q = P[j];
+      const int k = s - T.aoff[i], nh = Q.g.nh;
+      const double beta = ld_dbl(&A.st[j].beta);
+      double2 pv[3], acc[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double2 rv = ld2(Q.r + (size_t)c * nh + k), po = ld2(Q.p + (size_t)c * nh + k);
+        pv[c] = make_double2(fma(beta, po.x, rv.x), fma(beta, po.y, rv.y));
+        Q.p[(size_t)c * nh + k] = pv[c];
+        acc[c] = make_double2(4.0 * Q.m2 * pv[c].x, 4.0 * Q.m2 * pv[c].y);
+      }
+      hop_sum<NL, -1>(Q, 0, k, [&](int n, double2 v[3]) {
+        for (int c = 0; c < 3; c++) v[c] = ld2(Q.t + (size_t)c * nh + n);
+      }, acc);
+      double d = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        Q.ap[(size_t)c * nh + k] = acc[c];
+        d = fma(pv[c].x, acc[c].x, d);
+        d = fma(pv[c].y, acc[c].y, d);
+      }
+      A.dot[Q.off + k] = d;
+    }
+    finish_chunk(A, P, T, [&](int j, double pAp) {
+      BState &S = A.st[j];
+      S.pAp = pAp;
+      S.alpha = S.rz / pAp;
+      S.itn += 1;
+    });
+    if (!grid_sync(A.glob, tmo)) return;
+    // ---- phase C: x += alpha p; r -= alpha Ap; |r|^2 ----
+    for (int s = T.c0 + threadIdx.x; s < T.c1; s += blockDim.x) {
+      const int i = find_prob(T.aoff, T.na, s);
+      const int j = T.ids[i];
+      const BProb &Q = P[j];
+      const int k = s - T.aoff[i], nh = Q.g.nh, V = Q.g.V;
+      const double alpha = ld_dbl(&A.st[j].alpha);
+      double acc = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double2 pv = ld2(Q.p + (size_t)c * nh + k), av = ld2(Q.ap + (size_t)c * nh + k);
+        double2 xv = ld2(Q.x + (size_t)c * V + k), rv = ld2(Q.r + (size_t)c * nh + k);
+        xv.x = fma(alpha, pv.x, xv.x);
+        xv.y = fma(alpha, pv.y, xv.y);
+        rv.x = fma(-alpha, av.x, rv.x);
+        rv.y = fma(-alpha, av.y, rv.y);
+        Q.x[(size_t)c * V + k] = xv;
+        Q.r[(size_t)c * nh + k] = rv;
+        acc = fma(rv.x, rv.x, acc);
+        acc = fma(rv.y, rv.y, acc);
+      }
+      A.dot[Q.off + k] = acc;
+    }
+    finish_chunk(A, P, T, [&](int j, double r2) {
+      BState &S = A.st[j];
+      S.r2 = r2;
+      S.beta = r2 / S.rz;
+      S.rz = r2;
+      const int d = (!(S.itn < S.maxits && r2 > S.r2stop) || isnan(r2)) ? 1 : 0;
+      if (d) {
+        S.done = 1;
+        atomicSub(&A.glob->active, 1);
+      }
+    });
+    if (!grid_sync(A.glob, tmo)) return;
+  }
+}
+
+// per-problem and global state at the start of a solve (first node of the
+// captured graph, so that a relaunch starts from scratch)
+__global__ void batched_reset_kernel(BState *st, BGlobal *gl, int nprob, double r2req, int maxits) {
+  for (int j = threadIdx.x; j < nprob; j += blockDim.x) {
+    BState z;
+    memset(&z, 0, sizeof(z));
+    z.r2req = r2req;
+    z.maxits = maxits;
+    st[j] = z;
+  }
+  if (threadIdx.x == 0) {
+    gl->bar_count = 0;
+    gl->bar_gen = 0;
+    gl->err = 0;
+    gl->active = nprob;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side: arena, launch configuration (autotuned), graph
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct BatchCache {
+  void *arena = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  // autotuned (block, blocks per SM) per (nl, nprob, ntot) signature
+  std::map<std::vector<long>, std::pair<int, int>> tuned;
+  // captured graph for the last problem set
+  std::vector<long> gkey;
+  cudaGraphExec_t exec = nullptr;
+};
+BatchCache g_bc[64];
+
+int cache_of(BatchCache **out) {
+  int d = 0;
+  cudaGetDevice(&d);
+  if (d < 0 || d >= 64) return fail(QEXSTAG_ERR_ARG, "device out of range");
+  *out = &g_bc[d];
+  return QEXSTAG_OK;
+}
+
+template <int NL>
+int max_blocks(int block) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batched_cg_kernel<NL>, block, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+}  // namespace
+
+struct BatchRun {
+  int nl, nprob, ntot;
+  BProb *dprobs;
+  BState *dst;
+  BGlobal *dglob;
+  double *ddot;
+  double *dpart;  // kMaxBatch * max grid doubles
+  std::vector<BProb> hprobs;
+};
+
+// Upload the problem table for a grid of nb blocks and return the kernel
+// arguments.
+static int batched_args(const BatchRun &R, int nb, cudaStream_t s, BArgs *out) {
+  BArgs A;
+  A.probs = R.dprobs;
+  A.st = R.dst;
+  A.glob = R.dglob;
+  A.dot = R.ddot;
+  A.part = R.dpart;
+  A.part_stride = nb;
+  A.nprob = R.nprob;
+  A.ntot = R.ntot;
+  A.timeout_cycles = 4000000000LL;  // ~2 s at the boost clock
+  QS_CUDA(cudaMemcpyAsync(R.dprobs, R.hprobs.data(), sizeof(BProb) * R.nprob, cudaMemcpyHostToDevice, s));
+  QS_CUDA(cudaStreamSynchronize(s));
+  *out = A;
+  return QEXSTAG_OK;
+}
+
+// enqueue reset + the cooperative persistent kernel on s (capturable)
+static int enqueue_batched(const BatchRun &R, const BArgs &A, int nb, int block, cudaStream_t s, double r2req,
+                           int maxits) {
+  batched_reset_kernel<<<1, 128, 0, s>>>(R.dst, R.dglob, R.nprob, r2req, maxits);
+  QS_LAUNCH_CHECK();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nb);
+  cfg.blockDim = dim3(block);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = (R.nl == 8) ? cudaLaunchKernelEx(&cfg, batched_cg_kernel<8>, A)
+                              : cudaLaunchKernelEx(&cfg, batched_cg_kernel<4>, A);
+  if (e != cudaSuccess) return cuda_fail(e, "cooperative launch of batched_cg_kernel");
+  note_launch(2);
+  return QEXSTAG_OK;
+}
+
+static int launch_batched(const BatchRun &R, int block, int per_sm, cudaStream_t s, double r2req, int maxits) {
+  const int nb = num_sms() * per_sm;
+  BArgs A;
+  int rc = batched_args(R, nb, s, &A);
+  if (rc) return rc;
+  if ((rc = enqueue_batched(R, A, nb, block, s, r2req, maxits))) return rc;
+  QS_CUDA(cudaStreamSynchronize(s));
+  return QEXSTAG_OK;
+}
+
+// The solve as a CUDA graph: [reset, persistent kernel], captured once per
+// problem set and launch configuration and relaunched after that.  Returns
+// 1 in *used when the graph ran, 0 when capture was refused and the kernels
+// were launched directly instead.
+static int graph_batched(BatchCache *bc, const BatchRun &R, int block, int per_sm, double r2req, int maxits,
+                         int *used) {
+  std::vector<long> key{block, per_sm, R.nl, R.nprob, R.ntot, maxits};
+  long rbits;
+  std::memcpy(&rbits, &r2req, sizeof(rbits));
+  key.push_back(rbits);
+  for (const BProb &q : R.hprobs) {
+    key.push_back((long)q.u);
+    key.push_back((long)q.b);
+    key.push_back((long)q.x);
+    key.push_back((long)(q.m2 * 1e12));
+  }
+  cudaStream_t s = bc->stream;
+  if (!(bc->exec && bc->gkey == key)) {
+    if (bc->exec) cudaGraphExecDestroy(bc->exec);
+    bc->exec = nullptr;
+    bc->gkey.clear();
+    const int nb = num_sms() * per_sm;
+    BArgs A;
+    int rc = batched_args(R, nb, s, &A);
+    if (rc) return rc;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = enqueue_batched(R, A, nb, block, s, r2req, maxits);
+      e = cudaStreamEndCapture(s, &graph);
+    }
+    if (e == cudaSuccess && rc == QEXSTAG_OK && graph) e = cudaGraphInstantiate(&bc->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess || rc != QEXSTAG_OK || !bc->exec) {
+      cudaGetLastError();
+      bc->exec = nullptr;
+      *used = 0;
+      return launch_batched(R, block, per_sm, s, r2req, maxits);
+    }
+    bc->gkey = key;
+  }
+  QS_CUDA(cudaGraphLaunch(bc->exec, s));
+  note_launch(2);
+  QS_CUDA(cudaStreamSynchronize(s));
+  *used = 1;
+  return QEXSTAG_OK;
+}
+
+static int tune(BatchCache *bc, const BatchRun &R, double r2req, int *block, int *per_sm) {
+  std::vector<long> key{R.nl, R.nprob, R.ntot};
+  auto it = bc->tuned.find(key);
+  if (it != bc->tuned.end()) {
+    *block = it->second.first;
+    *per_sm = it->second.second;
+    return QEXSTAG_OK;
+  }
+  // candidates: block size x resident blocks per SM; each timed over a
+  // fixed number of iterations, the fastest kept
+  double best = 1e30;
+  int bb = 256, bp = 1;
+  cudaEvent_t e0, e1;
+  QS_CUDA(cudaEventCreate(&e0));
+  QS_CUDA(cudaEventCreate(&e1));
+  for (int blk : {128, 256, 512, 1024}) {
+    const int mx = (R.nl == 8) ? max_blocks<8>(blk) : max_blocks<4>(blk);
+    for (int ps = 1; ps <= std::min(mx, 32 * 128 / blk); ps++) {
+      cudaEventRecord(e0, bc->stream);
+      int rc = launch_batched(R, blk, ps, bc->stream, r2req, 12);
+      cudaEventRecord(e1, bc->stream);
+      cudaEventSynchronize(e1);
+      if (rc) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+      BGlobal hg;
+      QS_CUDA(cudaMemcpy(&hg, R.dglob, sizeof(hg), cudaMemcpyDeviceToHost));
+      if (hg.err) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return fail(QEXSTAG_ERR_TIMEOUT, "batched solve: a grid barrier timed out");
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        bb = blk;
+        bp = ps;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  bc->tuned[key] = {bb, bp};
+  *block = bb;
+  *per_sm = bp;
+  return QEXSTAG_OK;
+}
+
+int solve_batched(int nprob, qexstag_links_s *const *gs, const double *mass, double2 *const *x,
+                  const double2 *const *b, const qexstag_solver_params *p, int *iters, double *r2_out,
+                  qexstag_solver_stats *st, int *tuned_block, int *tuned_per_sm, int *graph_used) {
+  BatchCache *bc;
+  int rc = cache_of(&bc);
+  if (rc) return rc;
+  if (!bc->stream) QS_CUDA(cudaStreamCreateWithFlags(&bc->stream, cudaStreamNonBlocking));
+  const int nl = gs[0]->nl;
+  BatchRun R;
+  R.nl = nl;
+  R.nprob = nprob;
+  R.hprobs.resize(nprob);
+  int ntot = 0;
+  size_t vec_bytes = 0;
+  for (int j = 0; j < nprob; j++) {
+    vec_bytes += sizeof(double2) * 3 * (size_t)gs[j]->l->g.nh * 4;
+    ntot += gs[j]->l->g.nh;
+  }
+  R.ntot = ntot;
+  const size_t part_bytes = sizeof(double) * (size_t)kMaxBatch * num_sms() * 32;
+  const size_t bytes = vec_bytes + sizeof(double) * (size_t)ntot + sizeof(BProb) * kMaxBatch +
+                       sizeof(BState) * kMaxBatch + sizeof(BGlobal) + part_bytes + 8192;
+  if (bc->bytes < bytes) {
+    if (bc->arena) {
+      cudaDeviceSynchronize();
+      cudaFree(bc->arena);
+      bc->arena = nullptr;
+      bc->bytes = 0;
+      if (bc->exec) cudaGraphExecDestroy(bc->exec);
+      bc->exec = nullptr;
+      bc->gkey.clear();
+    }
+    cudaError_t e = cudaMalloc(&bc->arena, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(QEXSTAG_ERR_ALLOC, "batched solve: device allocation failed");
+    }
+    bc->bytes = bytes;
+  }
+  char *a = (char *)bc->arena;
+  auto take = [&](size_t n) {
+    char *q = a;
+    a += (n + 255) & ~(size_t)255;
+    return q;
+  };
+  R.dprobs = (BProb *)take(sizeof(BProb) * kMaxBatch);
+  R.dst = (BState *)take(sizeof(BState) * kMaxBatch);
+  R.dglob = (BGlobal *)take(sizeof(BGlobal));
+  R.ddot = (double *)take(sizeof(double) * (size_t)ntot);
+  R.dpart = (double *)take(part_bytes);
+  int off = 0;
+  for (int j = 0; j < nprob; j++) {
+    const Geom &g = gs[j]->l->g;
+    BProb &q = R.hprobs[j];
+    std::memset(&q, 0, sizeof(q));
+    q.g = g;
+    q.u = gs[j]->u64;
+    q.b = b[j];
+    q.x = x[j];
+    const size_t vb = sizeof(double2) * 3 * (size_t)g.nh;
+    q.r = (double2 *)take(vb);
+    q.p = (double2 *)take(vb);
+    q.ap = (double2 *)take(vb);
+    q.t = (double2 *)take(vb);
+    q.m2 = mass[j] * mass[j];
+    q.off = off;
+    off += g.nh;
+  }
+  // the batch runs on its own stream, ordered after the caller's work
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  const int maxits = p->maxits > 0 ? p->maxits : 50000;
+  int block = 256, per_sm = 1;
+  if ((rc = tune(bc, R, p->r2req, &block, &per_sm))) return rc;
+  *tuned_block = block;
+  *tuned_per_sm = per_sm;
+  if ((rc = graph_batched(bc, R, block, per_sm, p->r2req, maxits, graph_used))) return rc;
+  BGlobal hg;
+  QS_CUDA(cudaMemcpy(&hg, R.dglob, sizeof(hg), cudaMemcpyDeviceToHost));
+  if (hg.err) return fail(QEXSTAG_ERR_TIMEOUT, "batched solve: a grid barrier timed out");
+  std::vector<BState> hs(nprob);
+  QS_CUDA(cudaMemcpy(hs.data(), R.dst, sizeof(BState) * nprob, cudaMemcpyDeviceToHost));
+  int status = QEXSTAG_OK;
+  // FP64 true residuals; defect-correct any problem above its target
+  // (solveXX, stagSolve.nim:330-421)
+  for (int j = 0; j < nprob; j++) {
+    qexstag_links_s *g = gs[j];
+    const Geom &geo = g->l->g;
+    const int nh = geo.nh;
+    int its = hs[j].itn;
+    if (hs[j].b2 == 0.0) {
+      iters[j] = 0;
+      if (r2_out) r2_out[j] = 0.0;
+      continue;
+    }
+    if (std::isnan(hs[j].r2)) return fail(QEXSTAG_ERR_NAN, "batched solve: NaN residual");
+    void *prho, *pt, *py;
+    const size_t vb = sizeof(double2) * 3 * (size_t)nh;
+    if ((rc = g->ws.get(kSlotDcRho, vb, &prho)) || (rc = g->ws.get(kSlotTmpOdd, vb, &pt)) ||
+        (rc = g->ws.get(kSlotDcY, vb, &py)))
+      return rc;
+    VecD rho{(double2 *)prho, nh}, t{(double2 *)pt, nh}, y{(double2 *)py, nh};
+    VecD xj{x[j], geo.V};
+    double r2 = 0;
+    for (int pass = 0;; pass++) {
+      if ((rc = schur64(g, 0, rho, cv(xj), t, mass[j] * mass[j])) ||
+          (rc = vsub(rho, CVecD{b[j], geo.V}, cv(rho), nh)) || (rc = vnorm2(cv(rho), nh, &r2)))
+        return rc;
+      if (r2 <= p->r2req * hs[j].b2 || its >= maxits || pass >= 4) break;
+      CgOut o{};
+      if ((rc = cg64(g, 0, mass[j] * mass[j], cv(rho), y, p->r2req * hs[j].b2 / r2, maxits - its, &o)))
+        return rc;
+      its += o.iterations;
+      st->outer_iterations += 1;
+      if ((rc = vaxpy(xj, 1.0, cv(y), nh))) return rc;
+    }
+    iters[j] = its;
+    st->iterations += its;
+    const double rel = r2 / hs[j].b2;
+    if (r2_out) r2_out[j] = rel;
+    st->r2 = std::max(st->r2, rel);
+    if (r2 > p->r2req * hs[j].b2) status = QEXSTAG_NOT_CONVERGED;
+  }
+  return status;
+}
+
+}  // namespace qs
