@@ -245,10 +245,18 @@ def run_ours(args, dims):
     dom = {"fp64": "fp64", "fp32+fp64": "fp32", "fp16+fp64": "fp16"}[best]
     k = kt[dom]
     peak, peak_kind = measured_peaks()
+    # DRAM bytes (read + write) of one Schur call = its two half sweeps, from
+    # the ncu captures summarised in profiles/dslash_schur_fat_naik_32x32x32x32.md
+    # (32^4; per-launch traffic scales with the site count)
+    ncu_traffic_32 = {"fp64": 1233229000 + 5634048 + 1258927000 + 7406080,
+                      "fp32": 515961088 + 7234048 + 528527616 + 5271808,
+                      "fp16": 260101632 + 6382592 + 268475392 + 6029568}
+    traffic = ncu_traffic_32[dom] * nh / 524288
     roof = {"kernel": f"Schur operator, {dom} fat+Naik (two Dslash half sweeps)", "bound": "hbm",
             "achieved": round(k["GBps"], 1), "peak": peak, "unit": "GB/s",
             "frac": round(k["GBps"] / peak, 4), "peak_source": peak_kind,
-            "traffic": None, "bytes_per_even_site": k["bytes_per_even_site"],
+            "traffic": traffic, "traffic_unit": "bytes per Schur call (ncu, scaled from 32^4)",
+            "bytes_per_even_site": k["bytes_per_even_site"],
             "seconds_per_call": k["seconds"],
             "all_precisions": {n: {"GBps": round(v["GBps"], 1), "frac": round(v["GBps"] / peak, 4),
                                    "GFLOPs": round(v["GFLOPs"], 1), "us": round(v["seconds"] * 1e6, 1)}
