@@ -94,7 +94,10 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """One process per GPU (torchrun): every rank solves its own replica, so
+    the only collectives are the barriers around the timed region and the
+    max over ranks of the timings."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -102,7 +105,7 @@ def dist_setup():
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return ws, rank, local
 
 
@@ -117,7 +120,8 @@ def max_over_ranks(v, ws):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -144,7 +148,9 @@ def cpu_sample(dims, g, b, iters, fp64_iters):
 
 
 def run_reference(args, dims):
-    ws, rank, _ = dist_setup()
+    # the CPU reference arm runs on rank 0 alone; no process group is needed
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     g, b = make_inputs(dims, 0)

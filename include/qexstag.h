@@ -145,6 +145,12 @@ int qexstag_links_destroy(qexstag_links *g);
    so an HMC update of U is seen by the next solve; with device copies the
    caller calls this after changing the links. */
 int qexstag_links_update(qexstag_links *g, const double *links, int mem);
+/* QEX's rephase (src/physics/stagD.nim:106-114): multiply the handle's links
+   by the staggered phases [8,9,11,0] and the antiperiodic time boundary
+   signs (setBC, src/gauge/gaugeUtils.nim:133-140; for three-hop long links
+   the product of their three one-hop signs).  Applying it twice restores
+   the links, so it folds phases in and out; reduced copies are rebuilt. */
+int qexstag_links_rephase(qexstag_links *g);
 /* 1 when the handle uses 12-real long links in its reduced precisions. */
 int qexstag_links_recon12(const qexstag_links *g);
 

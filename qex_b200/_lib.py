@@ -72,6 +72,7 @@ SIGNATURES = {
     "qexstag_links_destroy": (I, [P]),
     "qexstag_links_recon12": (I, [P]),
     "qexstag_links_update": (I, [P, P, I]),
+    "qexstag_links_rephase": (I, [P]),
     "qexstag_stagD2": (I, [P, I, P, P, D, D, I]),
     "qexstag_stagD": (I, [P, I, P, P, D, D, D, I]),
     "qexstag_D": (I, [P, P, P, D, I]),

@@ -21,6 +21,7 @@ int solve_multishift(qexstag_links_s *g, int nmass, double2 *const *xs, const do
 int apply_D(qexstag_links_s *g, double2 *r, const double2 *x, double m, double sc);
 int stagD_par(qexstag_links_s *g, int par, double2 *r, const double2 *x, double m, double sc,
               double a);
+int rephase_links(qexstag_links_s *g);
 
 int Workspace::get(int slot, size_t bytes, void **out) {
   auto it = bufs.find(slot);
@@ -329,6 +330,14 @@ int qexstag_links_update(qexstag_links *g, const double *links, int mem) {
   if ((rc = upload_links(g, links, mem))) return rc;
   free_low_links(g->low);
   if ((rc = build_low_links(g))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_rephase(qexstag_links *g) {
+  int rc;
+  if ((rc = check_links(g))) return rc;
+  if ((rc = rephase_links(g))) return rc;
   QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
 }

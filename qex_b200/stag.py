@@ -183,6 +183,11 @@ class Staggered:
         ptr, mem = _ptr(links)
         L.check(self._lib.qexstag_links_update(self.handle, ptr, mem), "links_update")
 
+    def rephase(self) -> None:
+        """QEX's rephase: fold the staggered phases and boundary signs into
+        (or out of) the operator's links."""
+        L.check(self._lib.qexstag_links_rephase(self.handle), "links_rephase")
+
     @property
     def recon12(self) -> bool:
         return bool(self._lib.qexstag_links_recon12(self.handle))

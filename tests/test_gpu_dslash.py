@@ -124,3 +124,32 @@ def test_argument_errors(cuda):
     assert e.value.code == L.ERR_ARG
     lib = L.load()
     assert lib.qexstag_links_create(lay.handle, 5, None, 0, 1.0, None) == L.ERR_ARG
+
+
+@pytest.mark.parametrize("naik", [False, True])
+def test_rephase_on_device(cuda, naik):
+    """rephase of unphased links gives the operator of the phased links
+    (oracle's setBC + stagPhase); a second rephase restores them."""
+    dims = (8, 4, 6, 8)
+    V = F.volume(dims)
+    if naik:
+        rng = np.random.default_rng(4)
+        raw = F.interleave(F.fat_from_su3(F.warm_su3(4 * V, 0.3, rng), rng).reshape(4, V, 3, 3),
+                           F.warm_su3(4 * V, 0.3, rng).reshape(4, V, 3, 3))
+    else:
+        raw = F.gauge_warm(dims, 0.3, 4)
+    s = S.Staggered(S.Layout(dims), raw)
+    s.rephase()
+    o = O.Oracle(dims, O.apply_phases(dims, raw))
+    x = F.gaussian_vector(V, 9)
+    a, b = np.zeros_like(x), np.zeros_like(x)
+    s.D(a, x, 0.1)
+    o.D(b, x, 0.1)
+    assert rel(a, b) < TOL
+    if naik:
+        assert s.recon12
+    s.rephase()
+    o2 = O.Oracle(dims, raw)
+    o2.D(b, x, 0.1)
+    s.D(a, x, 0.1)
+    assert rel(a, b) < TOL
