@@ -80,7 +80,8 @@ typedef struct {
   double r2req;
   int maxits;
   int sloppy;          /* QEXSTAG_SLOPPY_* */
-  double delta;        /* reliable-update threshold for sloppy solves (0: 0.1) */
+  double delta;        /* reliable-update threshold for sloppy solves
+                          (0: 0.1 for SINGLE, 0.3 for HALF) */
   int verbosity;
   int use_prev_soln;   /* solve(): start from the x passed in */
   int reserved[6];

@@ -281,6 +281,18 @@ __device__ __forceinline__ bool mx_halt(const MxState *st) { return st->done || 
 // registers.  (Splitting a site's forward and backward hops over two threads
 // was slower: 3640-3720 GB/s.)
 
+// Format of the sloppy solver's vectors p and t for a link precision: the
+// same as the links, except that with 16-bit links the vectors may be kept
+// in FP32 (QS_HALF_VEC_BITS = 32), trading a few percent of traffic for the
+// iterations that 16-bit vectors cost.
+#ifndef QS_HALF_VEC_BITS
+#define QS_HALF_VEC_BITS 16
+#endif
+template <int PREC>
+struct VecPrec {
+  static constexpr int v = (PREC == kF16 && QS_HALF_VEC_BITS == 32) ? kF32 : PREC;
+};
+
 struct DslashArgsLo {
   Geom g;
   int po;
@@ -299,7 +311,7 @@ struct DslashArgsLo {
   double *dot_out;      // RED == 2
 };
 
-template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
+template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
 __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel(const DslashArgsLo A) {
   if (A.halt != nullptr && mx_halt(A.halt)) return;
   const Geom &g = A.g;
@@ -317,7 +329,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
       af[c] = make_float2(0.f, 0.f);
       al[c] = make_float2(0.f, 0.f);
     }
-    if (INIT) load_vec_cg<PREC>(A.xs, A.sstride, k, xsv);
+    if (INIT) load_vec_cg<VP>(A.xs, A.sstride, k, xsv);
 #pragma unroll
     for (int l = 0; l < NL; l++) {
       const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
@@ -326,8 +338,8 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
       const int jf = nbr_half(g, x, lex, mu, len);
       const int jb = nbr_half(g, x, lex, mu, -len);
       float2 v[3], w[3], uf[9], ub[9];
-      load_vec<PREC>(A.xin, A.istride, jf, v);
-      load_vec<PREC>(A.xin, A.istride, jb, w);
+      load_vec<VP>(A.xin, A.istride, jf, v);
+      load_vec<VP>(A.xin, A.istride, jb, w);
       if (is_long) {
         if (R12) {
           load_long12<PREC>(A.L, f, out_base + k, V, long_sign_fwd(g, x, mu), uf);
@@ -408,12 +420,12 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
 // resident blocks (occupancy from the runtime, so that no partial wave idles
 // SMs: on 32^4 two waves gave 5208 GB/s, 1.5 waves 4437); the FP32 kernel is
 // at the copy bandwidth with 4 blocks per SM.
-template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
+template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
 static int lo_grid(int nh) {
   static int resident = 0;  // one per kernel instantiation
   if (resident == 0) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, R12>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, R12>,
                                                       kBlock, 0) != cudaSuccess ||
         n < 1) {
       cudaGetLastError();
@@ -428,14 +440,14 @@ static int lo_grid(int nh) {
   return (int)(g < 1 ? 1 : g);
 }
 
-template <int PREC, int NL, int HOP, int INIT, int RED, int OUTP>
+template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP>
 static void launch_lo(const DslashArgsLo &A, int) {
   if (NL == 8 && A.L.recon12) {
-    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 1>
-        <<<lo_grid<PREC, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, 0, stream()>>>(A);
+    dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>
+        <<<lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, 0, stream()>>>(A);
   } else {
-    dslash_lo_kernel<PREC, NL, HOP, INIT, RED, OUTP, 0>
-        <<<lo_grid<PREC, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, 0, stream()>>>(A);
+    dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>
+        <<<lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, 0, stream()>>>(A);
   }
   note_launch();
 }
@@ -445,14 +457,15 @@ static void launch_lo(const DslashArgsLo &A, int) {
 //   which 1: ap = 4 m2 p - (2D)_{par,q} t      (out: FP32, hop -1, pAp)
 template <int PREC, int NL>
 static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red) {
+  constexpr int VP = VecPrec<PREC>::v;
   if (which == 0) {
-    launch_lo<PREC, NL, 1, 0, 0, PREC>(A, grid);
+    launch_lo<PREC, VP, NL, 1, 0, 0, VP>(A, grid);
   } else if (red == 1) {
-    launch_lo<PREC, NL, -1, 1, 1, kF32>(A, grid);
+    launch_lo<PREC, VP, NL, -1, 1, 1, kF32>(A, grid);
   } else if (red == 2) {
-    launch_lo<PREC, NL, -1, 1, 2, kF32>(A, grid);
+    launch_lo<PREC, VP, NL, -1, 1, 2, kF32>(A, grid);
   } else {
-    launch_lo<PREC, NL, -1, 1, 0, kF32>(A, grid);
+    launch_lo<PREC, VP, NL, -1, 1, 0, kF32>(A, grid);
   }
   QS_LAUNCH_CHECK();
   return QEXSTAG_OK;
@@ -715,17 +728,18 @@ int check_interval(int nh);
 template <int PREC>
 static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req,
                       int maxits, double delta, CgOut *out, int *reliable) {
+  constexpr int VP = VecPrec<PREC>::v;  // format of p and t
   const Geom &geo = g->l->g;
   const int nh = geo.nh;
   Workspace &ws = g->ws;
   const size_t v64 = sizeof(double2) * 3 * (size_t)nh, v32 = sizeof(float2) * 3 * (size_t)nh;
-  const size_t vp = (PREC == kF32) ? v32 : sizeof(uint4) * (size_t)nh;
+  const size_t vp = (VP == kF32) ? v32 : sizeof(uint4) * (size_t)nh;
   void *pr, *pax, *prs, *pxs, *pap, *pp, *pt, *pt64, *pst;
   int rc;
   if ((rc = ws.get(kSlotMx0 + 0, v64, &pr)) || (rc = ws.get(kSlotMx0 + 1, v64, &pax)) ||
       (rc = ws.get(kSlotMx0 + 2, v32, &prs)) || (rc = ws.get(kSlotMx0 + 3, v32, &pxs)) ||
-      (rc = ws.get(kSlotMx0 + 4, v32, &pap)) || (rc = ws.get(kSlotMx0 + 5 + 2 * PREC, vp, &pp)) ||
-      (rc = ws.get(kSlotMx0 + 6 + 2 * PREC, vp, &pt)) || (rc = ws.get(kSlotMx0 + 9, v64, &pt64)) ||
+      (rc = ws.get(kSlotMx0 + 4, v32, &pap)) || (rc = ws.get(kSlotMx0 + 5 + 2 * VP, vp, &pp)) ||
+      (rc = ws.get(kSlotMx0 + 6 + 2 * VP, vp, &pt)) || (rc = ws.get(kSlotMx0 + 9, v64, &pt64)) ||
       (rc = ws.get(kSlotMx0 + 10, sizeof(MxState), &pst)))
     return rc;
   double2 *r = (double2 *)pr, *ax = (double2 *)pax;
@@ -743,7 +757,7 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   }
   const int grid = grid_for(nh, kBlock, 4);
   const int egrid = grid_for(nh, kBlock, 8);
-  mx_init_kernel<PREC><<<grid, kBlock, 0, stream()>>>(b.p, b.stride, x.p, r, rs, xs, pp, nh, st,
+  mx_init_kernel<VP><<<grid, kBlock, 0, stream()>>>(b.p, b.stride, x.p, r, rs, xs, pp, nh, st,
                                                       red_partials(), red_tickets());
   note_launch();
   QS_LAUNCH_CHECK();
@@ -751,9 +765,9 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   for (;;) {
     for (int i = 0; i < every; i++) {
       if ((rc = schur_lo(g, PREC, par, ap, pp, pt, m2, 1, st, st, nullptr))) return rc;
-      mx_update_kernel<PREC><<<grid, kBlock, 0, stream()>>>(rs, xs, ap, pp, nh, st, red_partials(),
+      mx_update_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, xs, ap, pp, nh, st, red_partials(),
                                                             red_tickets());
-      mx_p_kernel<PREC><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
+      mx_p_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
       note_launch(2);
     }
     QS_LAUNCH_CHECK();
@@ -766,8 +780,8 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
     if ((rc = schur64(g, par, VecD{ax, nh}, cv(x), VecD{(double2 *)pt64, nh}, m2))) return rc;
     mx_true_res_kernel<<<grid, kBlock, 0, stream()>>>(b.p, b.stride, ax, r, rs, nh, st, red_partials(),
                                                       red_tickets());
-    mx_rp_kernel<PREC><<<grid, kBlock, 0, stream()>>>(rs, pp, nh, st, red_partials(), red_tickets());
-    mx_p_reliable_kernel<PREC><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
+    mx_rp_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, pp, nh, st, red_partials(), red_tickets());
+    mx_p_reliable_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
     mx_clear_pending_kernel<<<1, 1, 0, stream()>>>(st);
     note_launch(4);
     QS_LAUNCH_CHECK();
@@ -850,7 +864,7 @@ int bench_schur(qexstag_links_s *g, int prec, int nrep, double m2, double *sec) 
   } else if (prec == 1) {
     fill_vec_kernel<kF32><<<grid, kBlock, 0, stream()>>>(pa, nh, 1u);
   } else {
-    fill_vec_kernel<kF16><<<grid, kBlock, 0, stream()>>>(pa, nh, 1u);
+    fill_vec_kernel<VecPrec<kF16>::v><<<grid, kBlock, 0, stream()>>>(pa, nh, 1u);
   }
   note_launch();
   QS_LAUNCH_CHECK();

@@ -709,7 +709,7 @@ int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nr
         const int mx = maxits - st->iterations;
         if (sloppy)
           rc = cg_mixed(g, 0, m2s, CVecD{r, nh}, VecD{d, nh}, 0.5 * r2stop / r2, mx, p->sloppy,
-                        p->delta > 0 ? p->delta : 0.1, &o, &rel);
+                        p->delta > 0 ? p->delta : (p->sloppy == QEXSTAG_SLOPPY_HALF ? 0.3 : 0.1), &o, &rel);
         else
           rc = cg64(g, 0, m2s, CVecD{r, nh}, VecD{d, nh}, 0.5 * r2stop / r2, mx, &o);
         if (rc) return rc;

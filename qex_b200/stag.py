@@ -117,7 +117,7 @@ class SolverParams:
     r2req: float = 1e-6
     maxits: int = 50000
     sloppySolve: int = L.SLOPPY_NONE
-    delta: float = 0.1
+    delta: float = 0.0  # reliable-update threshold; 0 = the library's default
     verbosity: int = 0
     usePrevSoln: bool = False
     # outputs
