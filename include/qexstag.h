@@ -255,6 +255,57 @@ int qexstag_force_solve(qexstag_links *g, double *psi, const double *phi, double
    consumes.  Layout as qexstag_force's f. */
 int qexstag_ferm_outer(qexstag_links *g, double *f, const double *psi, int mem);
 
+/* ---- HISQ link smearing (src/gauge/fat7l.nim, src/physics/hisqLinks.nim,
+   src/gauge/hisqsmear.nim) ----
+   Gauge fields here are the four directions of a link field:
+   double[4][V][3][3][2] on the host or double2[4][9][V] on the device, the
+   layouts of qexstag_links_create with nlinks = 4.  QEX smears links with
+   the staggered phases and boundary signs already folded in
+   (hmcAction.nim:540-555 calls setBC and stagPhase before smearing). */
+
+/* Fat7lCoefs (fat7l.nim:5-10) */
+typedef struct {
+  double one_link, three_staple, five_staple, seven_staple, lepage;
+} qexstag_fat7_coefs;
+/* HisqCoefs (hisqLinks.nim:3-8); reunit_eps is projectU's eps
+   (matrixFunctions.nim:340-351, 1e-20) */
+typedef struct {
+  qexstag_fat7_coefs fat7first, fat7second;
+  double naik;
+  double reunit_eps;
+} qexstag_hisq_coefs;
+/* setHisqFat7 (hisqLinks.nim:10-15) */
+void qexstag_fat7_coefs_set_hisq(qexstag_fat7_coefs *c, double f7lf, double naik);
+/* newHISQ (hisqsmear.nim:53-64): first level (lepage, 0), second level
+   (2 - lepage, naik), long-link coefficient -naik/24, reunit_eps 1e-20 */
+void qexstag_hisq_coefs_init(qexstag_hisq_coefs *c, double lepage, double naik);
+
+/* A smearing handle holds the device scratch of the staple sweeps (36 link
+   fields of 144 B per site, plus staging); it keeps a pointer to l. */
+typedef struct qexstag_smear_s qexstag_smear;
+int qexstag_smear_create(qexstag_layout *l, qexstag_smear **out);
+int qexstag_smear_destroy(qexstag_smear *s);
+/* makeImpLinks (fat7l.nim:70-154): fl = fat7 smearing of gf with one-link,
+   3-, 5-, 7-staple and Lepage terms; when naik != 0 and gf_long, ll are
+   non-NULL also ll_mu(x) = naik gf_long_mu(x) gf_long_mu(x+mu)
+   gf_long_mu(x+2mu). */
+int qexstag_fat7(qexstag_smear *s, const qexstag_fat7_coefs *c, const double *gf, double *fl,
+                 const double *gf_long, double *ll, double naik, int mem);
+/* projectU (matrixFunctions.nim:340-351) of every link: u = x (x^dag x +
+   eps)^(-1/2) */
+int qexstag_project_u(qexstag_smear *s, const double *x, double *u, double eps, int mem);
+/* HisqCoefs.smear (hisqLinks.nim:40-46): fat7 with fat7first, projectU, then
+   fat7 with fat7second and the Naik product of the projected links. */
+int qexstag_hisq_smear(qexstag_smear *s, const qexstag_hisq_coefs *c, const double *g, double *fat,
+                       double *lng, int mem);
+/* Smear thin links g into the fat+Naik handle (nlinks 8, same layout as s):
+   its list becomes [fat_0, long_0, ..., fat_3, long_3] as newStag3 builds it
+   from HISQ's outputs, and its reduced-precision copies are rebuilt.  The
+   projected links are unitary, not special unitary, so the long links keep
+   18 reals. */
+int qexstag_links_hisq(qexstag_links *g, qexstag_smear *s, const qexstag_hisq_coefs *c, const double *thin,
+                       int mem);
+
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */
 

@@ -22,8 +22,8 @@ _lib = None
 
 
 def build() -> Path:
-    src = HERE / "qexstag_oracle.c"
-    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+    srcs = [HERE / "qexstag_oracle.c", HERE / "smear_oracle.c"]
+    if not LIB.exists() or any(LIB.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB
 
@@ -65,6 +65,9 @@ def lib():
             "or_ferm_outer": (None, [P, P, P]),
             "or_force": (I, [P, P, P, D, D, I, DP]),
             "or_num_threads": (I, []),
+            "or_fat7": (None, [C.POINTER(C.c_int), DP, P, P, P, P, D]),
+            "or_project_u": (None, [C.c_long, P, P, D]),
+            "or_hisq_smear": (None, [C.POINTER(C.c_int), DP, DP, D, D, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(l, name)
@@ -198,3 +201,52 @@ class Oracle:
 
 def num_threads() -> int:
     return lib().or_num_threads()
+
+
+# ---- HISQ smearing (smear_oracle.c) ------------------------------------
+# coefficient order {oneLink, threeStaple, fiveStaple, sevenStaple, lepage}
+
+
+def hisq_fat7_coefs(f7lf: float, naik: float):
+    """setHisqFat7 (src/physics/hisqLinks.nim:10-15)."""
+    return [(1.0 + 3.0 * f7lf + naik) / 8.0, -1.0 / 16.0, 1.0 / 64.0, -1.0 / 384.0, -f7lf / 16.0]
+
+
+def hisq_coefs(lepage: float = 0.0, naik: float = 1.0):
+    """newHISQ (src/gauge/hisqsmear.nim:53-64): (first, second, naik)."""
+    return hisq_fat7_coefs(lepage, 0.0), hisq_fat7_coefs(2.0 - lepage, naik), -naik / 24.0
+
+
+def _coef(c):
+    return (C.c_double * 5)(*[float(v) for v in c])
+
+
+def fat7(dims, coefs, gf: np.ndarray, gfl: np.ndarray | None = None, naik: float = 0.0):
+    """makeImpLinks (src/gauge/fat7l.nim:70-154) on (4, V, 3, 3) fields;
+    returns fl, or (fl, ll) when gfl is given."""
+    gf = np.ascontiguousarray(gf, dtype=np.complex128)
+    fl = np.empty_like(gf)
+    if gfl is None:
+        lib().or_fat7(_dims(dims), _coef(coefs), _p(gf), _p(fl), None, None, 0.0)
+        return fl
+    gfl = np.ascontiguousarray(gfl, dtype=np.complex128)
+    ll = np.empty_like(gfl)
+    lib().or_fat7(_dims(dims), _coef(coefs), _p(gf), _p(fl), _p(gfl), _p(ll), naik)
+    return fl, ll
+
+
+def project_u(x: np.ndarray, eps: float = 1e-20) -> np.ndarray:
+    """projectU (src/maths/matrixFunctions.nim:340-351) of (..., 3, 3)."""
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.empty_like(x)
+    lib().or_project_u(x.size // 9, _p(x), _p(out), eps)
+    return out
+
+
+def hisq_smear(dims, g: np.ndarray, lepage: float = 0.0, naik: float = 1.0, eps: float = 1e-20):
+    """HisqCoefs.smear (src/physics/hisqLinks.nim:40-46): (fat, long)."""
+    first, second, cn = hisq_coefs(lepage, naik)
+    g = np.ascontiguousarray(g, dtype=np.complex128)
+    fl, ll = np.empty_like(g), np.empty_like(g)
+    lib().or_hisq_smear(_dims(dims), _coef(first), _coef(second), cn, eps, _p(g), _p(fl), _p(ll))
+    return fl, ll

@@ -51,6 +51,19 @@ class SolverStatsC(C.Structure):
     ]
 
 
+class Fat7CoefsC(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("one_link", "three_staple", "five_staple", "seven_staple", "lepage")]
+
+
+class HisqCoefsC(C.Structure):
+    _fields_ = [
+        ("fat7first", Fat7CoefsC),
+        ("fat7second", Fat7CoefsC),
+        ("naik", C.c_double),
+        ("reunit_eps", C.c_double),
+    ]
+
+
 P = C.c_void_p
 D = C.c_double
 I = C.c_int
@@ -91,6 +104,14 @@ SIGNATURES = {
     "qexstag_force_solve": (I, [P, P, P, D, P, P, I]),
     "qexstag_ferm_outer": (I, [P, P, P, I]),
     "qexstag_bench_schur": (I, [P, I, I, D, DP]),
+    "qexstag_fat7_coefs_set_hisq": (None, [P, D, D]),
+    "qexstag_hisq_coefs_init": (None, [P, D, D]),
+    "qexstag_smear_create": (I, [P, C.POINTER(P)]),
+    "qexstag_smear_destroy": (I, [P]),
+    "qexstag_fat7": (I, [P, P, P, P, P, P, D, I]),
+    "qexstag_project_u": (I, [P, P, P, D, I]),
+    "qexstag_hisq_smear": (I, [P, P, P, P, P, I]),
+    "qexstag_links_hisq": (I, [P, P, P, P, I]),
 }
 
 _lib = None
