@@ -89,40 +89,53 @@ __device__ __forceinline__ void m_dn(M3 &r, const M3 &a, const M3 &b) {
 
 // Site index of x + a*mu (periodic): lex moves by the wrapped step, the
 // parity flips with a odd (all L even).
+// (selects instead of indexing x[] with a runtime direction, which would put
+// the coordinates in local memory)
+__device__ __forceinline__ int pick(const int v[4], int d) {
+  return d == 0 ? v[0] : d == 1 ? v[1] : d == 2 ? v[2] : v[3];
+}
+// lex offset of moving a steps along mu from coordinate xm (periodic)
+__device__ __forceinline__ int lex_step(const Geom &g, const int x[4], int mu, int a) {
+  const int xm = pick(x, mu), Lm = pick(g.L, mu);
+  int y = xm + a;
+  if (y >= Lm) y -= Lm;
+  if (y < 0) y += Lm;
+  return (y - xm) * pick(g.stride, mu);
+}
 __device__ __forceinline__ int disp1(const Geom &g, const int x[4], int lex, int par, int mu, int a) {
-  int y = x[mu] + a;
-  if (y >= g.L[mu]) y -= g.L[mu];
-  if (y < 0) y += g.L[mu];
-  const int l = lex + (y - x[mu]) * g.stride[mu];
+  const int l = lex + lex_step(g, x, mu, a);
   return (l >> 1) + (((par ^ a) & 1) ? g.nh : 0);
 }
 // x + a*mu + b*nu, mu != nu
 __device__ __forceinline__ int disp2(const Geom &g, const int x[4], int lex, int par, int mu, int a, int nu,
                                      int b) {
-  int y = x[mu] + a, z = x[nu] + b;
-  if (y >= g.L[mu]) y -= g.L[mu];
-  if (y < 0) y += g.L[mu];
-  if (z >= g.L[nu]) z -= g.L[nu];
-  if (z < 0) z += g.L[nu];
-  const int l = lex + (y - x[mu]) * g.stride[mu] + (z - x[nu]) * g.stride[nu];
+  const int l = lex + lex_step(g, x, mu, a) + lex_step(g, x, nu, b);
   return (l >> 1) + (((par ^ a ^ b) & 1) ? g.nh : 0);
 }
 
 struct SiteCtx {
-  int x[4], lex, par, site;
+  int x[4], lex, par, site, mu;
 };
 
+// Block b works on direction b % 4 and parity (b / 4) % 2 of the chunk of
+// kSmBlock half-lattice sites b / 8, so the eight blocks that read each
+// other's links as neighbours run together and those reads hit L2 (with the
+// direction- or parity-major order every link is fetched from HBM again by a
+// later pass).
 __device__ __forceinline__ bool site_of_thread(const Geom &g, SiteCtx &c) {
-  c.site = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c.site >= g.V) return false;
-  c.par = c.site >= g.nh ? 1 : 0;
-  site_coords(g, c.par, c.site - c.par * g.nh, c.x, c.lex);
+  const int b = blockIdx.x;
+  c.mu = b & 3;
+  c.par = (b >> 2) & 1;
+  const int k = (b >> 3) * blockDim.x + threadIdx.x;
+  if (k >= g.nh) return false;
+  c.site = c.par * g.nh + k;
+  site_coords(g, c.par, k, c.x, c.lex);
   return true;
 }
 
 // S = U_nu(x) F(x+nu) U_nu(x+mu)^dag + U_nu(x-nu)^dag F(x-nu) U_nu(x-nu+mu).
-// The second factor of each product is streamed from memory row by row so
-// that at most two 3x3 matrices besides S are live.
+// Every factor is streamed from memory a row or column at a time, so only
+// the partial product t and S are live 3x3 matrices.
 __device__ __forceinline__ void staple(M3 &S, const Geom &g, const SiteCtx &c, int mu, int nu,
                                        const double2 *__restrict__ Un, const double2 *__restrict__ F) {
   const size_t V = (size_t)g.V;
@@ -130,20 +143,22 @@ __device__ __forceinline__ void staple(M3 &S, const Geom &g, const SiteCtx &c, i
   const int s_pm = disp1(g, c.x, c.lex, c.par, mu, 1);
   const int s_mn = disp1(g, c.x, c.lex, c.par, nu, -1);
   const int s_mnpm = disp2(g, c.x, c.lex, c.par, nu, -1, mu, 1);
-  M3 a, t;
-  // upper: t = U_nu(x) F(x+nu); S = t U_nu(x+mu)^dag
-  m_load(a, Un, V, c.site);
+  M3 t;
+  // upper: t = U_nu(x) F(x+nu) (column k of U times row k of F); S = t U_nu(x+mu)^dag
 #pragma unroll
   for (int e = 0; e < 9; e++) t.e[e] = make_double2(0.0, 0.0);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    double2 b[3];
+    double2 a[3], b[3];
 #pragma unroll
-    for (int j = 0; j < 3; j++) b[j] = __ldg(F + (size_t)(3 * k + j) * V + s_pn);
+    for (int j = 0; j < 3; j++) {
+      a[j] = __ldg(Un + (size_t)(3 * j + k) * V + c.site);
+      b[j] = __ldg(F + (size_t)(3 * k + j) * V + s_pn);
+    }
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-      for (int j = 0; j < 3; j++) t.e[3 * i + j] = cmadd(t.e[3 * i + j], a.e[3 * i + k], b[j]);
+      for (int j = 0; j < 3; j++) t.e[3 * i + j] = cmadd(t.e[3 * i + j], a[i], b[j]);
   }
 #pragma unroll
   for (int j = 0; j < 3; j++) {
@@ -158,19 +173,21 @@ __device__ __forceinline__ void staple(M3 &S, const Geom &g, const SiteCtx &c, i
       S.e[3 * i + j] = s;
     }
   }
-  // lower: t = U_nu(x-nu)^dag F(x-nu); S += t U_nu(x-nu+mu)
-  m_load(a, Un, V, s_mn);
+  // lower: t = U_nu(x-nu)^dag F(x-nu) (rows k of both); S += t U_nu(x-nu+mu)
 #pragma unroll
   for (int e = 0; e < 9; e++) t.e[e] = make_double2(0.0, 0.0);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    double2 b[3];
+    double2 a[3], b[3];
 #pragma unroll
-    for (int j = 0; j < 3; j++) b[j] = __ldg(F + (size_t)(3 * k + j) * V + s_mn);
+    for (int j = 0; j < 3; j++) {
+      a[j] = __ldg(Un + (size_t)(3 * k + j) * V + s_mn);
+      b[j] = __ldg(F + (size_t)(3 * k + j) * V + s_mn);
+    }
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-      for (int j = 0; j < 3; j++) t.e[3 * i + j] = cjmadd(t.e[3 * i + j], a.e[3 * k + i], b[j]);
+      for (int j = 0; j < 3; j++) t.e[3 * i + j] = cjmadd(t.e[3 * i + j], a[i], b[j]);
   }
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -210,10 +227,10 @@ __device__ __forceinline__ int third_dir(int mu, int nu, int r) {
 }
 
 // sweep 1: one-link term and 3-staples
-__global__ void __launch_bounds__(kSmBlock) fat7_three_kernel(const Fat7Args A) {
+__global__ void __launch_bounds__(kSmBlock, 3) fat7_three_kernel(const Fat7Args A) {
   SiteCtx c;
   if (!site_of_thread(A.g, c)) return;
-  const int mu = blockIdx.y;
+  const int mu = c.mu;
   const size_t V = (size_t)A.g.V;
   const double2 *Um = A.u + mu * A.ufs;
   M3 acc;
@@ -233,10 +250,10 @@ __global__ void __launch_bounds__(kSmBlock) fat7_three_kernel(const Fat7Args A) 
 }
 
 // sweep 2: Lepage staples and 5-staples of the stored 3-staples
-__global__ void __launch_bounds__(kSmBlock) fat7_five_kernel(const Fat7Args A) {
+__global__ void __launch_bounds__(kSmBlock, 3) fat7_five_kernel(const Fat7Args A) {
   SiteCtx c;
   if (!site_of_thread(A.g, c)) return;
-  const int mu = blockIdx.y;
+  const int mu = c.mu;
   const size_t V = (size_t)A.g.V;
   double2 *flm = A.fl + mu * A.ffs;
   M3 acc;
@@ -264,10 +281,10 @@ __global__ void __launch_bounds__(kSmBlock) fat7_five_kernel(const Fat7Args A) {
 }
 
 // sweep 3: 7-staples of the stored 5-staples
-__global__ void __launch_bounds__(kSmBlock) fat7_seven_kernel(const Fat7Args A) {
+__global__ void __launch_bounds__(kSmBlock, 3) fat7_seven_kernel(const Fat7Args A) {
   SiteCtx c;
   if (!site_of_thread(A.g, c)) return;
-  const int mu = blockIdx.y;
+  const int mu = c.mu;
   const size_t V = (size_t)A.g.V;
   double2 *flm = A.fl + mu * A.ffs;
   M3 acc;
@@ -292,7 +309,7 @@ __global__ void __launch_bounds__(kSmBlock)
     naik_kernel(Geom g, const double2 *__restrict__ u, size_t ufs, double2 *ll, size_t lfs, double naik) {
   SiteCtx c;
   if (!site_of_thread(g, c)) return;
-  const int mu = blockIdx.y;
+  const int mu = c.mu;
   const size_t V = (size_t)g.V;
   const double2 *U = u + mu * ufs;
   M3 a, b, t;
@@ -365,7 +382,8 @@ __global__ void __launch_bounds__(kSmBlock)
   m_store(out + mu * ofs, (size_t)V, s, w);
 }
 
-static dim3 sweep_grid(const Geom &g) { return dim3((unsigned)((g.V + kSmBlock - 1) / kSmBlock), 4, 1); }
+static dim3 sweep_grid(const Geom &g) { return dim3((unsigned)(8 * ((g.nh + kSmBlock - 1) / kSmBlock)), 1, 1); }
+static dim3 field_grid(const Geom &g) { return dim3((unsigned)((g.V + kSmBlock - 1) / kSmBlock), 4, 1); }
 
 // makeImpLinks on device fields: u (stride ufs between directions) -> fl
 // (stride ffs); s3/s5 scratch
@@ -412,7 +430,7 @@ int naik_dev(const Geom &g, const double2 *u, size_t ufs, double2 *ll, size_t lf
 }
 
 int project_u_dev(const Geom &g, const double2 *in, size_t ifs, double2 *out, size_t ofs, double eps) {
-  project_u_kernel<<<sweep_grid(g), kSmBlock, 0, stream()>>>(g.V, in, ifs, out, ofs, eps);
+  project_u_kernel<<<field_grid(g), kSmBlock, 0, stream()>>>(g.V, in, ifs, out, ofs, eps);
   note_launch();
   QS_LAUNCH_CHECK();
   return QEXSTAG_OK;
