@@ -306,6 +306,33 @@ int qexstag_hisq_smear(qexstag_smear *s, const qexstag_hisq_coefs *c, const doub
 int qexstag_links_hisq(qexstag_links *g, qexstag_smear *s, const qexstag_hisq_coefs *c, const double *thin,
                        int mem);
 
+/* ---- chain rule through the smearing (src/gauge/fat7lderiv.nim,
+   src/maths/matrixFunctions.nim:368-390, src/gauge/hisqsmear.nim:66-105) ----
+   Derivatives follow QEX's convention: for a chain C on an output field and
+   S = sum_x Re Tr C(x)^dagger out(x), the derivative with respect to an
+   input field U is the field f with dS = sum_x Re Tr dU(x)^dagger f(x). */
+
+/* fat7lDeriv (fat7lderiv.nim:122-331): deriv += derivative w.r.t. gauge of
+   sum Re Tr mid^dag fat7(gauge); when naik != 0 and llgauge, llmid, llderiv
+   are non-NULL also llderiv += derivative w.r.t. llgauge of
+   sum Re Tr llmid^dag naik llgauge(x) llgauge(x+mu) llgauge(x+2mu).  Like
+   QEX's, it adds to deriv and llderiv (which may be the same field when
+   llgauge == gauge). */
+int qexstag_fat7_deriv(qexstag_smear *s, const qexstag_fat7_coefs *c, const double *gauge, const double *mid,
+                       double *deriv, const double *llgauge, const double *llmid, double *llderiv, double naik,
+                       int mem);
+/* projectUderiv (matrixFunctions.nim:368-390) of every link: r = derivative
+   w.r.t. x of Re Tr chain^dag projectU(x), with u = projectU(x). */
+int qexstag_project_u_deriv(qexstag_smear *s, const double *u, const double *x, const double *chain, double *r,
+                            double eps, int mem);
+/* smearGetForce's chain rule (hisqsmear.nim:66-105): deriv = derivative
+   w.r.t. the thin links g of sum Re Tr (cfat^dag fat(g) + clong^dag long(g))
+   for the smearing of qexstag_hisq_smear.  Recomputes the forward smearing
+   of g.  cfat, clong are QEX's dsdsu, dsdsul (for the fermion force, its
+   outer products f1 and f3). */
+int qexstag_hisq_deriv(qexstag_smear *s, const qexstag_hisq_coefs *c, const double *g, const double *cfat,
+                       const double *clong, double *deriv, int mem);
+
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */
 

@@ -68,6 +68,10 @@ def lib():
             "or_fat7": (None, [C.POINTER(C.c_int), DP, P, P, P, P, D]),
             "or_project_u": (None, [C.c_long, P, P, D]),
             "or_hisq_smear": (None, [C.POINTER(C.c_int), DP, DP, D, D, P, P, P]),
+            "or_fat7_deriv": (None, [C.POINTER(C.c_int), DP, P, P, P, P, P, P, D]),
+            "or_project_u_deriv": (None, [C.c_long, P, P, P, P, D]),
+            "or_sylsolve": (None, [C.c_long, P, P, P]),
+            "or_hisq_deriv": (None, [C.POINTER(C.c_int), DP, DP, D, D, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(l, name)
@@ -230,7 +234,7 @@ def fat7(dims, coefs, gf: np.ndarray, gfl: np.ndarray | None = None, naik: float
         lib().or_fat7(_dims(dims), _coef(coefs), _p(gf), _p(fl), None, None, 0.0)
         return fl
     gfl = np.ascontiguousarray(gfl, dtype=np.complex128)
-    ll = np.empty_like(gfl)
+    ll = np.zeros_like(gfl)  # left untouched when naik == 0, as makeImpLinks does
     lib().or_fat7(_dims(dims), _coef(coefs), _p(gf), _p(fl), _p(gfl), _p(ll), naik)
     return fl, ll
 
@@ -250,3 +254,50 @@ def hisq_smear(dims, g: np.ndarray, lepage: float = 0.0, naik: float = 1.0, eps:
     fl, ll = np.empty_like(g), np.empty_like(g)
     lib().or_hisq_smear(_dims(dims), _coef(first), _coef(second), cn, eps, _p(g), _p(fl), _p(ll))
     return fl, ll
+
+
+
+def fat7_deriv(dims, coefs, gauge, mid, llgauge=None, llmid=None, naik: float = 0.0):
+    """fat7lDeriv (src/gauge/fat7lderiv.nim:122-331): derivative of
+    sum Re Tr mid^dag fat7(gauge) (+ llmid^dag naik-product(llgauge)) with
+    respect to gauge (and llgauge): (deriv, llderiv or None)."""
+    gauge = np.ascontiguousarray(gauge, dtype=np.complex128)
+    mid = np.ascontiguousarray(mid, dtype=np.complex128)
+    d = np.zeros_like(gauge)
+    if llgauge is None:
+        lib().or_fat7_deriv(_dims(dims), _coef(coefs), _p(gauge), _p(mid), _p(d), None, None, None, 0.0)
+        return d, None
+    llgauge = np.ascontiguousarray(llgauge, dtype=np.complex128)
+    llmid = np.ascontiguousarray(llmid, dtype=np.complex128)
+    dl = np.zeros_like(gauge)
+    lib().or_fat7_deriv(_dims(dims), _coef(coefs), _p(gauge), _p(mid), _p(d), _p(llgauge), _p(llmid), _p(dl),
+                        naik)
+    return d, dl
+
+
+def project_u_deriv(u, x, chain, eps: float = 1e-20):
+    """projectUderiv (src/maths/matrixFunctions.nim:368-390)."""
+    u, x, chain = (np.ascontiguousarray(a, dtype=np.complex128) for a in (u, x, chain))
+    r = np.empty_like(x)
+    lib().or_project_u_deriv(x.size // 9, _p(u), _p(x), _p(chain), _p(r), eps)
+    return r
+
+
+def sylsolve(a, c):
+    """x with a x + x a = c (src/maths/projUderiv.nim:96-145)."""
+    a, c = (np.ascontiguousarray(v, dtype=np.complex128) for v in (a, c))
+    x = np.empty_like(c)
+    lib().or_sylsolve(c.size // 9, _p(a), _p(c), _p(x))
+    return x
+
+
+def hisq_deriv(dims, g, cfat, clong, lepage: float = 0.0, naik: float = 1.0, eps: float = 1e-20,
+               coefs=None):
+    """smearGetForce's chain rule (src/gauge/hisqsmear.nim:66-105): the
+    derivative of sum Re Tr (cfat^dag fat(g) + clong^dag long(g)) w.r.t. g.
+    coefs = (first, second, naik) overrides newHISQ(lepage, naik)."""
+    first, second, cn = coefs if coefs is not None else hisq_coefs(lepage, naik)
+    g, cfat, clong = (np.ascontiguousarray(a, dtype=np.complex128) for a in (g, cfat, clong))
+    d = np.empty_like(g)
+    lib().or_hisq_deriv(_dims(dims), _coef(first), _coef(second), cn, eps, _p(g), _p(cfat), _p(clong), _p(d))
+    return d

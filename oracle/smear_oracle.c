@@ -20,6 +20,14 @@
  *  - newHISQ:                    src/gauge/hisqsmear.nim:53-64
  *  - projectU (Cayley-Hamilton): src/maths/matrixFunctions.nim:118-150,
  *                                165-212, 340-351
+ *  - symStaple / symStapleDeriv: src/gauge/smearutil.nim:3-56
+ *  - fat7lDeriv (with Naik):     src/gauge/fat7lderiv.nim:122-331
+ *  - projectUderiv, sylsolve:    src/maths/matrixFunctions.nim:360-390,
+ *                                src/maths/projUderiv.nim:96-145
+ *  - smearGetForce's chain rule: src/gauge/hisqsmear.nim:66-105
+ * The chain rule is pinned by QEX's own check (hisqsmear.nim:126-168):
+ * finite differences of sum Re Tr (C^dag fat + Cl^dag long) along random
+ * directions, for one-link-only, fat7-only and full HISQ coefficients.
  *
  * Layout: a gauge field is double[4][V][3][3][2] (direction, QEX V=1 site
  * index, row-major 3x3, re/im); coefficient arrays are
@@ -275,4 +283,318 @@ void or_hisq_smear(const int L[4], const double *first, const double *second, do
   or_fat7(L, second, t2, fl, t2, ll, naik);
   free(t1);
   free(t2);
+}
+
+/* ------------------------------------------------------------------ */
+/* chain rule through the smearing                                     */
+/* ------------------------------------------------------------------ */
+/* Convention (QEX's, src/gauge/hisqsmear.nim:111-168): for a chain C on an
+   output field and S = sum_x Re Tr C(x)^dagger out(x), the derivative with
+   respect to an input field U is the field f with dS = sum Re Tr dU^dagger f. */
+
+static void m_dd(double *r, const double *a, const double *b) { /* a^dag b^dag */
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double re = 0, im = 0;
+      for (int k = 0; k < 3; k++) {
+        const double *p = a + 2 * (3 * k + i), *q = b + 2 * (3 * j + k);
+        re += p[0] * q[0] - p[1] * q[1];
+        im += -p[0] * q[1] - p[1] * q[0];
+      }
+      r[2 * (3 * i + j)] = re;
+      r[2 * (3 * i + j) + 1] = im;
+    }
+}
+static void f_dd(const SGeo *s, double *r, const double *a, const double *b) {
+#pragma omp parallel for
+  for (long i = 0; i < s->V; i++) m_dd(r + 18 * i, a + 18 * i, b + 18 * i);
+}
+
+/* symStaple (src/gauge/smearutil.nim:3-20): s += alp [g1 g2(x+d1) g1(x+d2)^dag
+   + (g1^dag g2 g1(x+d2))(x-d1)], g1 the side field of direction d1, g2 the
+   middle field of direction d2 */
+static void sym_staple(const SGeo *s, double *st, double alp, const double *g1, const double *g2, int d1, int d2,
+                       double *w) {
+  const long n = 18 * s->V;
+  double *s1 = w, *s2 = w + n, *t = w + 2 * n, *tm = w + 3 * n, *sm = w + 4 * n;
+  shift_m(s, s1, g1, d2, 1);
+  shift_m(s, s2, g2, d1, 1);
+  f_dn(s, t, g1, g2);
+  f_nn(s, tm, t, s1);
+  shift_m(s, sm, tm, d1, -1);
+  f_nn(s, t, g1, s2);
+  f_nd(s, tm, t, s1);
+  f_axpy(s, st, alp, tm);
+  f_axpy(s, st, alp, sm);
+}
+
+/* symStapleDeriv (src/gauge/smearutil.nim:22-56): with chain c on
+   symStaple(g1, g2), f1 += derivative w.r.t. g1 and f2 += derivative w.r.t.
+   g2 */
+static void sym_staple_deriv(const SGeo *s, double *f1, double *f2, const double *g1, const double *g2, int d1,
+                             int d2, const double *c, double *w) {
+  const long n = 18 * s->V;
+  double *s1 = w, *s2 = w + n, *sc = w + 2 * n, *t = w + 3 * n, *tm1 = w + 4 * n, *tm2 = w + 5 * n,
+         *sm = w + 6 * n, *u = w + 7 * n;
+  shift_m(s, s1, g1, d2, 1);
+  shift_m(s, s2, g2, d1, 1);
+  shift_m(s, sc, c, d1, 1);
+  f_dn(s, t, g1, c);
+  f_nn(s, tm1, t, s1);      /* g1^dag c s1 */
+  f_dn(s, t, g2, g1);
+  f_nn(s, tm2, t, sc);      /* g2^dag g1 s */
+  f_dn(s, t, c, g1);
+  f_nn(s, u, t, s2);        /* c^dag g1 s2 */
+  f_axpy(s, tm2, 1.0, u);
+  f_nn(s, t, g2, s1);
+  f_nd(s, u, t, sc);
+  f_axpy(s, f1, 1.0, u);    /* g2 s1 s^dag */
+  f_nn(s, t, c, s1);
+  f_nd(s, u, t, s2);
+  f_axpy(s, f1, 1.0, u);    /* c s1 s2^dag */
+  f_nn(s, t, g1, sc);
+  f_nd(s, u, t, s1);
+  f_axpy(s, f2, 1.0, u);    /* g1 s s1^dag */
+  shift_m(s, sm, tm1, d1, -1);
+  f_axpy(s, f2, 1.0, sm);
+  shift_m(s, sm, tm2, d2, -1);
+  f_axpy(s, f1, 1.0, sm);
+}
+
+/* fat7lDeriv (src/gauge/fat7lderiv.nim:122-331): deriv += d/d gauge of
+   sum Re Tr mid^dag fat7(gauge); when naik != 0 and ll fields are given,
+   llderiv += d/d llgauge of sum Re Tr llmid^dag naik U(x)U(x+mu)U(x+2mu).
+   All fields [4][V][18]. */
+void or_fat7_deriv(const int L[4], const double *coef, const double *gauge, const double *mid, double *deriv,
+                   const double *llgauge, const double *llmid, double *llderiv, double naik) {
+  SGeo s;
+  sgeo_init(&s, L);
+  const long n = 18 * s.V;
+  const double coefL = coef[4], coef1 = coef[0] - 6.0 * coefL, coef3 = coef[1], coef5 = coef[2], coef7 = coef[3];
+  const int have5 = (coef5 != 0.0) || (coef7 != 0.0) || (coefL != 0.0);
+  const int have3 = (coef3 != 0.0) || have5;
+  const double *g[4], *md[4];
+  double *dv[4];
+  for (int d = 0; d < 4; d++) {
+    g[d] = gauge + d * n;
+    md[d] = mid + d * n;
+    dv[d] = deriv + d * n;
+  }
+  double *stpl3 = (double *)calloc(4 * n, sizeof(double));
+  double *mid5 = (double *)calloc(4 * n, sizeof(double));
+  double *stpl5 = (double *)malloc(sizeof(double) * n);
+  double *mid3 = (double *)malloc(sizeof(double) * n);
+  double *w = (double *)malloc(sizeof(double) * 8 * n);
+  for (int sig = 0; sig < 4; sig++) {
+    if (have5) {
+      for (int mu = 0; mu < 4; mu++) {
+        if (mu == sig) continue;
+        memset(stpl3 + mu * n, 0, sizeof(double) * n);
+        sym_staple(&s, stpl3 + mu * n, 1.0, g[mu], g[sig], mu, sig, w);
+        memset(mid5 + mu * n, 0, sizeof(double) * n);
+      }
+      for (int rho = 0; rho < 4; rho++) {
+        if (rho == sig) continue;
+        memset(stpl5, 0, sizeof(double) * n);
+        if (coef7 != 0.0) {
+          for (int mu = 0; mu < 4; mu++) {
+            if (mu == sig || mu == rho) continue;
+            for (int nu = 0; nu < 4; nu++) {
+              if (nu == sig || nu == rho || nu == mu) continue;
+              sym_staple(&s, stpl5, 1.0, g[nu], stpl3 + mu * n, nu, sig, w);
+            }
+          }
+          for (long i = 0; i < n; i++) stpl5[i] *= coef7;
+        }
+        memset(mid3, 0, sizeof(double) * n);
+        if (coefL != 0.0) f_axpy(&s, stpl5, coefL, stpl3 + rho * n);
+        if (coefL != 0.0 || coef7 != 0.0) sym_staple_deriv(&s, dv[rho], mid3, g[rho], stpl5, rho, sig, md[sig], w);
+        if (coefL != 0.0) f_axpy(&s, mid5 + rho * n, coefL, mid3);
+        for (long i = 0; i < n; i++) mid3[i] *= coef7;
+        f_axpy(&s, mid3, coef5, md[sig]);
+        for (int mu = 0; mu < 4; mu++) {
+          if (mu == sig || mu == rho) continue;
+          for (int nu = 0; nu < 4; nu++) {
+            if (nu == sig || nu == rho || nu == mu) continue;
+            sym_staple_deriv(&s, dv[mu], mid5 + nu * n, g[mu], stpl3 + nu * n, mu, sig, mid3, w);
+          }
+        }
+      }
+    }
+    if (have3) {
+      memset(mid3, 0, sizeof(double) * n);
+      for (int mu = 0; mu < 4; mu++) {
+        if (mu == sig) continue;
+        for (long i = 0; i < n; i++) stpl5[i] = coef3 * md[sig][i] + (have5 ? mid5[mu * n + i] : 0.0);
+        sym_staple_deriv(&s, dv[mu], mid3, g[mu], g[sig], mu, sig, stpl5, w);
+      }
+      f_axpy(&s, dv[sig], 1.0, mid3);
+    }
+    if (coef1 != 0.0) f_axpy(&s, dv[sig], coef1, md[sig]);
+  }
+  if (naik != 0.0 && llgauge && llmid && llderiv) {
+    double *sa = w, *tm1 = w + n, *sm = w + 2 * n, *tm2 = w + 3 * n, *sb = w + 4 * n, *t = w + 5 * n;
+    for (int mu = 0; mu < 4; mu++) {
+      const double *lg = llgauge + mu * n, *lm = llmid + mu * n;
+      double *ld = llderiv + mu * n;
+      shift_m(&s, sa, lg, mu, 1);          /* U(x+mu) */
+      f_dn(&s, tm1, lg, lm);               /* U^dag mid */
+      shift_m(&s, sm, tm1, mu, -1);
+      f_dd(&s, tm2, sa, lg);               /* U(x+mu)^dag U^dag */
+      shift_m(&s, sb, tm2, mu, 1);
+      f_nd(&s, t, sm, sa);
+      f_axpy(&s, ld, naik, t);
+      f_dn(&s, tm1, lg, sm);
+      shift_m(&s, sm, tm1, mu, -1);
+      f_nn(&s, t, lm, sb);
+      f_axpy(&s, t, 1.0, sm);
+      f_axpy(&s, ld, naik, t);
+    }
+  }
+  free(stpl3);
+  free(mid5);
+  free(stpl5);
+  free(mid3);
+  free(w);
+  free(s.coord);
+}
+
+/* 3x3 inverse through the adjugate */
+static void m_adjugate(double *r, const double *x) {
+#define XR(i, j) x[2 * (3 * (i) + (j))]
+#define XI(i, j) x[2 * (3 * (i) + (j)) + 1]
+  /* r_ij = x_ab x_cd - x_ef x_gh with the index pattern of the cofactors */
+  static const int P[9][8] = {{1, 1, 2, 2, 1, 2, 2, 1}, {2, 1, 0, 2, 2, 2, 0, 1}, {0, 1, 1, 2, 0, 2, 1, 1},
+                              {1, 2, 2, 0, 1, 0, 2, 2}, {2, 2, 0, 0, 2, 0, 0, 2}, {0, 2, 1, 0, 0, 0, 1, 2},
+                              {1, 0, 2, 1, 1, 1, 2, 0}, {2, 0, 0, 1, 2, 1, 0, 0}, {0, 0, 1, 1, 0, 1, 1, 0}};
+  for (int e = 0; e < 9; e++) {
+    const int *p = P[e];
+    const double ar = XR(p[0], p[1]), ai = XI(p[0], p[1]), br = XR(p[2], p[3]), bi = XI(p[2], p[3]);
+    const double cr = XR(p[4], p[5]), ci = XI(p[4], p[5]), dr = XR(p[6], p[7]), di = XI(p[6], p[7]);
+    r[2 * e] = (ar * br - ai * bi) - (cr * dr - ci * di);
+    r[2 * e + 1] = (ar * bi + ai * br) - (cr * di + ci * dr);
+  }
+#undef XR
+#undef XI
+}
+
+static void m_inverse(double *r, const double *x) {
+  double ad[18];
+  m_adjugate(ad, x);
+  /* det = sum_k x_0k ad_k0 */
+  double dr = 0, di = 0;
+  for (int k = 0; k < 3; k++) {
+    const double *a = x + 2 * k, *b = ad + 2 * (3 * k);
+    dr += a[0] * b[0] - a[1] * b[1];
+    di += a[0] * b[1] + a[1] * b[0];
+  }
+  const double nn = dr * dr + di * di, ir = dr / nn, ii = -di / nn;
+  for (int e = 0; e < 9; e++) {
+    const double a = ad[2 * e], b = ad[2 * e + 1];
+    r[2 * e] = a * ir - b * ii;
+    r[2 * e + 1] = a * ii + b * ir;
+  }
+}
+
+/* sylsolve (src/maths/projUderiv.nim:96-145, 3x3 branch): x with
+   a x + x a = c, from the adjugate of a and its invariants (a Hermitian
+   positive here, so the invariants are taken real) */
+static void sylsolve3(double *x, const double *a, const double *c) {
+  double ad[18], ac[18], ca[18], aca[18], adc[18], cad[18], adcad[18];
+  m_adjugate(ad, a);
+  const double t = a[0] + a[8] + a[16];
+  const double s = ad[0] + ad[8] + ad[16];
+  double r = 0;
+  for (int k = 0; k < 3; k++) r += a[2 * k] * ad[2 * (3 * k)] - a[2 * k + 1] * ad[2 * (3 * k) + 1];
+  m_nn(ac, a, c);
+  m_nn(ca, c, a);
+  m_nn(aca, ac, a);
+  m_nn(adc, ad, c);
+  m_nn(cad, c, ad);
+  m_nn(adcad, adc, ad);
+  const double c2 = 1.0 / (2.0 * (s * t - r));
+  const double c0 = c2 * (s + t * t), c1 = c2 * (t / r), c4 = c2 * t;
+  for (int i = 0; i < 18; i++)
+    x[i] = c0 * c[i] + c1 * adcad[i] + c2 * (aca[i] - adc[i] - cad[i]) - c4 * (ac[i] + ca[i]);
+}
+
+/* inverse square root of x^dagger x + eps (projectUrsqrt,
+   matrixFunctions.nim:340-346) */
+static void rsqrt_xdx(double *z, const double *x, double eps) {
+  /* projectU computes x z; recover z = x^-1 (x z) would lose accuracy, so
+     repeat its inner steps */
+  double t[18], t2[18];
+  m_dn(t, x, x);
+  t[0] += eps;
+  t[8] += eps;
+  t[16] += eps;
+  m_nn(t2, t, t);
+  const double tr = t[0] + t[8] + t[16];
+  const double p2 = t2[0] + t2[8] + t2[16];
+  double ad[18];
+  m_adjugate(ad, t);
+  double det = 0;
+  for (int k = 0; k < 3; k++) det += t[2 * k] * ad[2 * (3 * k)] - t[2 * k + 1] * ad[2 * (3 * k) + 1];
+  double l0, l1, l2;
+  eigs3(&l0, &l1, &l2, tr, p2, det);
+  const double s0 = sqrt(fabs(l0)), s1 = sqrt(fabs(l1)), s2 = sqrt(fabs(l2));
+  const double u = s0 + s1 + s2, w = s0 * s1 * s2;
+  const double di = 1.0 / (w * (s0 + s1) * (s0 + s2) * (s1 + s2));
+  const double c0 = (w * u * u + l0 * s0 * (l1 + l2) + l1 * s1 * (l0 + l2) + l2 * s2 * (l0 + l1)) * di;
+  const double c1 = -(tr * u + w) * di, c2 = u * di;
+  for (int i = 0; i < 18; i++) z[i] = c1 * t[i] + c2 * t2[i];
+  z[0] += c0;
+  z[8] += c0;
+  z[16] += c0;
+}
+
+/* projectUderiv (matrixFunctions.nim:368-390): r = d/dx of
+   Re Tr chain^dagger projectU(x), with u = projectU(x).  r may alias chain. */
+static void project_u_deriv1(double *r, const double *u, const double *x, const double *chain, double eps) {
+  double z[18], y[18], t1[18], t2[18], cz[18];
+  rsqrt_xdx(z, x, eps);
+  m_inverse(y, z);
+  m_nn(cz, chain, z);
+  m_dn(t1, u, cz);
+  sylsolve3(t2, y, t1);
+  for (int i = 0; i < 9; i++) {  /* t1 = t2 + t2^dagger */
+    const int p = i / 3, q = i % 3, e = 3 * q + p;
+    t1[2 * i] = t2[2 * i] + t2[2 * e];
+    t1[2 * i + 1] = t2[2 * i + 1] - t2[2 * e + 1];
+  }
+  m_nn(t2, x, t1);
+  for (int i = 0; i < 18; i++) r[i] = cz[i] - t2[i];
+}
+
+void or_project_u_deriv(long n, const double *u, const double *x, const double *chain, double *r, double eps) {
+#pragma omp parallel for
+  for (long i = 0; i < n; i++) project_u_deriv1(r + 18 * i, u + 18 * i, x + 18 * i, chain + 18 * i, eps);
+}
+
+void or_sylsolve(long n, const double *a, const double *c, double *x) {
+  for (long i = 0; i < n; i++) sylsolve3(x + 18 * i, a + 18 * i, c + 18 * i);
+}
+
+/* the chain rule of HisqCoefs' smearing (smearGetForce's smearedForce,
+   src/gauge/hisqsmear.nim:66-105): deriv = d/dg of
+   sum Re Tr (cfat^dag fat(g) + clong^dag long(g)) */
+void or_hisq_deriv(const int L[4], const double *first, const double *second, double naik, double eps,
+                   const double *g, const double *cfat, const double *clong, double *deriv) {
+  const long V = (long)L[0] * L[1] * L[2] * L[3];
+  const long n = 4 * 18 * V;
+  double *v = (double *)malloc(sizeof(double) * n);
+  double *w = (double *)malloc(sizeof(double) * n);
+  double *f = (double *)calloc(n, sizeof(double));
+  double *fll = (double *)calloc(n, sizeof(double));
+  or_fat7(L, first, g, v, NULL, NULL, 0.0);
+  or_project_u(4 * V, v, w, eps);
+  or_fat7_deriv(L, second, w, cfat, f, w, clong, fll, naik);
+  for (long i = 0; i < n; i++) f[i] += fll[i];
+  or_project_u_deriv(4 * V, w, v, f, f, eps);
+  memset(deriv, 0, sizeof(double) * n);
+  or_fat7_deriv(L, first, g, f, deriv, NULL, NULL, NULL, 0.0);
+  free(v);
+  free(w);
+  free(f);
+  free(fll);
 }

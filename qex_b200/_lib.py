@@ -112,6 +112,9 @@ SIGNATURES = {
     "qexstag_project_u": (I, [P, P, P, D, I]),
     "qexstag_hisq_smear": (I, [P, P, P, P, P, I]),
     "qexstag_links_hisq": (I, [P, P, P, P, I]),
+    "qexstag_fat7_deriv": (I, [P, P, P, P, P, P, P, P, D, I]),
+    "qexstag_project_u_deriv": (I, [P, P, P, P, P, D, I]),
+    "qexstag_hisq_deriv": (I, [P, P, P, P, P, P, I]),
 }
 
 _lib = None

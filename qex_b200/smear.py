@@ -115,6 +115,39 @@ class Smear:
         L.check(self._lib.qexstag_hisq_smear(self.handle, C.byref(cc), _ptr(g)[0], _ptr(fl, True)[0],
                                              _ptr(ll, True)[0], mem), "hisq_smear")
 
+    def fat7Deriv(self, deriv, gauge, mid, coef: Fat7lCoefs, llderiv=None, llgauge=None, llmid=None,
+                  naik: float = 0.0) -> None:
+        """fat7lDeriv (fat7lderiv.nim:122-331): adds to deriv (and llderiv) the
+        derivative of sum Re Tr (mid^dag fat7(gauge) + llmid^dag naik-product(llgauge))."""
+        fields = [deriv, gauge, mid] + ([llderiv, llgauge, llmid] if llderiv is not None else [])
+        for f in fields:
+            _check_gauge(self.l, f)
+        mem = _mem_of(*fields)
+        cc = coef.c()
+        ld = _ptr(llderiv, True)[0] if llderiv is not None else None
+        lg = _ptr(llgauge)[0] if llgauge is not None else None
+        lm = _ptr(llmid)[0] if llmid is not None else None
+        L.check(self._lib.qexstag_fat7_deriv(self.handle, C.byref(cc), _ptr(gauge)[0], _ptr(mid)[0],
+                                             _ptr(deriv, True)[0], lg, lm, ld, float(naik), mem), "fat7_deriv")
+
+    def projectUderiv(self, r, u, x, chain, eps: float = 1e-20) -> None:
+        """projectUderiv (matrixFunctions.nim:368-390) per link."""
+        for f in (r, u, x, chain):
+            _check_gauge(self.l, f)
+        mem = _mem_of(r, u, x, chain)
+        L.check(self._lib.qexstag_project_u_deriv(self.handle, _ptr(u)[0], _ptr(x)[0], _ptr(chain)[0],
+                                                  _ptr(r, True)[0], float(eps), mem), "project_u_deriv")
+
+    def smearDeriv(self, coef: HisqCoefs, g, cfat, clong, deriv) -> None:
+        """smearGetForce's chain rule (hisqsmear.nim:66-105): deriv = d/dg of
+        sum Re Tr (cfat^dag fat(g) + clong^dag long(g))."""
+        for f in (g, cfat, clong, deriv):
+            _check_gauge(self.l, f)
+        mem = _mem_of(g, cfat, clong, deriv)
+        cc = coef.c()
+        L.check(self._lib.qexstag_hisq_deriv(self.handle, C.byref(cc), _ptr(g)[0], _ptr(cfat)[0], _ptr(clong)[0],
+                                             _ptr(deriv, True)[0], mem), "hisq_deriv")
+
     def smear_into(self, stag: Staggered, coef: HisqCoefs, g) -> None:
         """Smear thin links g into a fat+Naik operator's link list and rebuild
         its reduced-precision copies."""

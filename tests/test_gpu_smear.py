@@ -124,3 +124,78 @@ def test_smear_errors(cuda):
     assert lib.qexstag_hisq_smear(None, None, None, None, None, 0) == L.ERR_ARG
     with pytest.raises(ValueError):
         sm.projectU(np.empty((4, 10, 3, 3), complex), g)
+
+
+# ---- chain rule ------------------------------------------------------------
+
+def chains(g, seed):
+    rng = np.random.default_rng(seed)
+    return tuple(rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape) for _ in range(2))
+
+
+@pytest.mark.parametrize("dims", SHAPES[:2])
+def test_fat7_deriv_matches_oracle(cuda, dims):
+    g = thin(dims, 4)
+    gl = thin(dims, 5, 0.3)
+    ch, chl = chains(g, 6)
+    sm = SM.Smear(S.Layout(dims))
+    c = SM.Fat7lCoefs(*GENERIC)
+    # without Naik; adds to what deriv holds
+    pre = chains(g, 7)[0]
+    d = pre.copy()
+    sm.fat7Deriv(d, g, ch, c)
+    od, _ = O.fat7_deriv(dims, GENERIC, g, ch)
+    assert rel(d - pre, od) < TOL
+    # Naik on a separate field
+    d, dl = np.zeros_like(g), np.zeros_like(g)
+    sm.fat7Deriv(d, g, ch, c, dl, gl, chl, -0.3)
+    od, odl = O.fat7_deriv(dims, GENERIC, g, ch, gl, chl, -0.3)
+    assert rel(d, od) < TOL and rel(dl, odl) < TOL
+    # Naik on the same field (HISQ's second level)
+    d = np.zeros_like(g)
+    sm.fat7Deriv(d, g, ch, c, d, g, chl, -0.3)
+    assert rel(d, od + O.fat7_deriv(dims, GENERIC, g, ch * 0, g, chl, -0.3)[1]) < TOL
+
+
+def test_project_u_deriv_matches_oracle(cuda):
+    dims = (4, 4, 4, 6)
+    x = O.fat7(dims, O.hisq_coefs()[0], thin(dims, 3))
+    u = O.project_u(x)
+    ch, _ = chains(x, 9)
+    sm = SM.Smear(S.Layout(dims))
+    r = np.empty_like(x)
+    sm.projectUderiv(r, u, x, ch)
+    assert rel(r, O.project_u_deriv(u, x, ch)) < 1e-11
+
+
+DERIV_CASES = {
+    "hisq": (None, None),
+    "fat7": ((0.0, 0.0), (0.0, 0.0)),
+    "lepage+naik": (None, [0.5, -0.1, 0.2, -0.03, 0.04]),
+}
+
+
+@pytest.mark.parametrize("case", sorted(DERIV_CASES))
+@pytest.mark.parametrize("dims", SHAPES)
+def test_hisq_deriv_matches_oracle(cuda, dims, case):
+    torch = cuda
+    g = thin(dims, 6)
+    cf, cl = chains(g, 11)
+    coef = SM.newHISQ()
+    first, second, cn = O.hisq_coefs()
+    f2, s2 = DERIV_CASES[case]
+    if f2 is not None:
+        first, second, cn = O.hisq_fat7_coefs(*f2), O.hisq_fat7_coefs(*s2), 0.0
+        coef.fat7first, coef.fat7second, coef.naik = SM.Fat7lCoefs(*first), SM.Fat7lCoefs(*second), 0.0
+    elif s2 is not None:
+        second, cn = s2, -0.1
+        coef.fat7second, coef.naik = SM.Fat7lCoefs(*second), cn
+    od = O.hisq_deriv(dims, g, cf, cl, coefs=(first, second, cn))
+    sm = SM.Smear(S.Layout(dims))
+    d = np.empty_like(g)
+    sm.smearDeriv(coef, g, cf, cl, d)
+    assert rel(d, od) < 1e-11
+    if dims == SHAPES[0]:
+        dd = torch.empty_like(S.to_device_links(g))
+        sm.smearDeriv(coef, S.to_device_links(g), S.to_device_links(cf), S.to_device_links(cl), dd)
+        assert np.array_equal(S.to_host_links(dd), d)

@@ -98,3 +98,84 @@ def test_terms_are_separable():
     total = O.fat7(dims, c, g)
     parts = sum(O.fat7(dims, [c[i] if j == i else 0.0 for j in range(5)], g) for i in range(5))
     assert np.abs(total - parts).max() < 1e-14
+
+
+# ---- chain rule (fat7lDeriv, projectUderiv, smearGetForce) ----------------
+
+def rdot(a, b):
+    return float(np.sum((np.conj(a) * b).real))
+
+
+def test_sylsolve_solves_the_sylvester_equation():
+    rng = np.random.default_rng(2)
+    a = rng.normal(size=(50, 3, 3)) + 1j * rng.normal(size=(50, 3, 3))
+    a = a @ np.conj(np.swapaxes(a, -1, -2)) + 0.1 * np.eye(3)
+    c = rng.normal(size=(50, 3, 3)) + 1j * rng.normal(size=(50, 3, 3))
+    x = O.sylsolve(a, c)
+    assert np.abs(a @ x + x @ a - c).max() < 1e-12 * np.abs(c).max()
+
+
+def test_project_u_deriv_finite_differences():
+    rng = np.random.default_rng(4)
+    x = rng.normal(size=(40, 3, 3)) + 1j * rng.normal(size=(40, 3, 3))
+    ch = rng.normal(size=x.shape) + 1j * rng.normal(size=x.shape)
+    dx = rng.normal(size=x.shape) + 1j * rng.normal(size=x.shape)
+    r = O.project_u_deriv(O.project_u(x), x, ch)
+    eps = 1e-6
+    fd = (rdot(ch, O.project_u(x + eps * dx)) - rdot(ch, O.project_u(x - eps * dx))) / (2 * eps)
+    assert abs(fd - rdot(dx, r)) < 1e-8 * abs(fd)
+
+
+HISQ_CASES = {
+    # QEX's own check (hisqsmear.nim:158-168): one-link only, fat7 without
+    # Naik, full HISQ
+    "oneLink": ([1.0, 0, 0, 0, 0], [1.0, 0, 0, 0, 0], 0.0),
+    "fat7": (O.hisq_fat7_coefs(0, 0), O.hisq_fat7_coefs(0, 0), 0.0),
+    "hisq": O.hisq_coefs(),
+    "lepage+naik": (O.hisq_coefs()[0], [0.5, -0.1, 0.2, -0.03, 0.04], -0.1),
+}
+
+
+@pytest.mark.parametrize("case", sorted(HISQ_CASES))
+def test_hisq_chain_rule_finite_differences(case):
+    """d/dt S(g + t dg) at t = 0 by central differences (eps 1e-5) against
+    sum Re Tr dg^dag deriv, S = sum Re Tr (C^dag fat + Cl^dag long)."""
+    dims = (4, 4, 4, 4)
+    rng = np.random.default_rng(3)
+    g = O.apply_phases(dims, F.gauge_warm(dims, 0.5, 3))
+    ch = rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape)
+    chl = rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape)
+    dg = rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape)
+    first, second, cn = coefs = HISQ_CASES[case]
+
+    def S(u):
+        w = O.project_u(O.fat7(dims, first, u))
+        fl, ll = O.fat7(dims, second, w, w, cn)
+        return rdot(ch, fl) + rdot(chl, ll)
+
+    d = O.hisq_deriv(dims, g, ch, chl, coefs=coefs)
+    eps = 1e-5
+    fd = (S(g + eps * dg) - S(g - eps * dg)) / (2 * eps)
+    assert abs(fd - rdot(dg, d)) < 1e-7 * abs(fd)
+
+
+def test_fat7_deriv_finite_differences_with_naik():
+    dims = (4, 4, 4, 6)
+    rng = np.random.default_rng(8)
+    g = O.apply_phases(dims, F.gauge_warm(dims, 0.5, 3))
+    gl = O.apply_phases(dims, F.gauge_warm(dims, 0.4, 5))
+    ch = rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape)
+    chl = rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape)
+    dg = rng.normal(size=g.shape) + 1j * rng.normal(size=g.shape)
+    c = [0.3, 0.2, -0.1, 0.05, 0.07]
+
+    def S(u, ul):
+        fl, ll = O.fat7(dims, c, u, ul, -0.3)
+        return rdot(ch, fl) + rdot(chl, ll)
+
+    d, dl = O.fat7_deriv(dims, c, g, ch, gl, chl, -0.3)
+    eps = 1e-5
+    fd = (S(g + eps * dg, gl) - S(g - eps * dg, gl)) / (2 * eps)
+    assert abs(fd - rdot(dg, d)) < 1e-8 * abs(fd)
+    fd = (S(g, gl + eps * dg) - S(g, gl - eps * dg)) / (2 * eps)
+    assert abs(fd - rdot(dg, dl)) < 1e-8 * abs(fd)
