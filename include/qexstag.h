@@ -332,6 +332,17 @@ int qexstag_project_u_deriv(qexstag_smear *s, const double *u, const double *x, 
    outer products f1 and f3). */
 int qexstag_hisq_deriv(qexstag_smear *s, const qexstag_hisq_coefs *c, const double *g, const double *cfat,
                        const double *clong, double *deriv, int mem);
+/* The staggered fermion force with HISQ smearing (QEX's force with
+   StaggeredSmearing == "HISQ", hmcAction.nim:851-885 and fermForce
+   723-790): smear the thin links into g (nlinks 8; its links are replaced),
+   solve stagD2ee(m^2) y = phi_e (stagForceSolve), form the outer products
+   f1, f3 of psi = (4y, (2D)_oe 4y) with the odd-site sign, take the chain
+   rule through the smearing, and return f_mu = projectTAH(ff_mu U_mu^dag)
+   on the thin links: the f QEX passes to addForce(gf, 0.25*dtau, f).  thin
+   and f are 4-direction gauge fields, phi a full-lattice colour vector. */
+int qexstag_hisq_force(qexstag_links *g, qexstag_smear *s, const qexstag_hisq_coefs *c, const double *thin,
+                       double *f, const double *phi, double m, const qexstag_solver_params *p,
+                       qexstag_solver_stats *st, int mem);
 
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */

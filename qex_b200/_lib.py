@@ -115,6 +115,7 @@ SIGNATURES = {
     "qexstag_fat7_deriv": (I, [P, P, P, P, P, P, P, P, D, I]),
     "qexstag_project_u_deriv": (I, [P, P, P, P, P, D, I]),
     "qexstag_hisq_deriv": (I, [P, P, P, P, P, P, I]),
+    "qexstag_hisq_force": (I, [P, P, P, P, P, P, D, P, P, I]),
 }
 
 _lib = None

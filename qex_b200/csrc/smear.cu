@@ -199,8 +199,8 @@ int project_u_dev(const Geom &g, const double2 *in, size_t ifs, double2 *out, si
 namespace qs {
 
 // HisqCoefs.smear into device fields fat (stride ffs) and long (stride lfs)
-static int hisq_dev(qexstag_smear_s *s, const qexstag_hisq_coefs &c, const double2 *g, double2 *fat, size_t ffs,
-                    double2 *lng, size_t lfs) {
+int hisq_dev(qexstag_smear_s *s, const qexstag_hisq_coefs &c, const double2 *g, double2 *fat, size_t ffs,
+             double2 *lng, size_t lfs) {
   const Geom &geo = s->l->g;
   const size_t fs = (size_t)9 * geo.V;
   void *pt1, *pw;

@@ -343,4 +343,8 @@ inline bool finite_coefs(const qexstag_fat7_coefs &c) {
          std::isfinite(c.seven_staple) && std::isfinite(c.lepage);
 }
 
+// HisqCoefs.smear of device links g into fat (stride ffs) and long (stride lfs)
+int hisq_dev(qexstag_smear_s *s, const qexstag_hisq_coefs &c, const double2 *g, double2 *fat, size_t ffs,
+             double2 *lng, size_t lfs);
+
 }  // namespace qs

@@ -505,6 +505,34 @@ static int hisq_deriv_dev(qexstag_smear_s *s, const qexstag_hisq_coefs &c, const
   return fat7_adj_dev(geo, c.fat7first, g, fs, dw, fs, nullptr, 0, 0.0, s3, s5, t7, m3, d, fs, false);
 }
 
+// F_d(x) = projectTAH(ff_d(x) U_d(x)^dag)   (fermForce's last step,
+// hmcAction.nim:780-790; projectTAH: matrixFunctions.nim:414-419)
+__global__ void __launch_bounds__(kSmBlock)
+    tah_times_adj_kernel(int V, const double2 *__restrict__ ff, const double2 *__restrict__ u, double2 *out,
+                         size_t fs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  const size_t off = blockIdx.y * fs;
+  M3 a, b, m;
+  m_load(a, ff + off, (size_t)V, s);
+  m_load(b, u + off, (size_t)V, s);
+  m_nd(m, a, b);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const double2 p = m.e[3 * i + j], q = m.e[3 * j + i];
+      a.e[3 * i + j] = make_double2(0.5 * (p.x - q.x), 0.5 * (p.y + q.y));
+    }
+  const double tr = (a.e[0].y + a.e[4].y + a.e[8].y) * (1.0 / 3.0);
+  a.e[0].y -= tr;
+  a.e[4].y -= tr;
+  a.e[8].y -= tr;
+  m_store(out + off, (size_t)V, s, a);
+}
+
+enum ForceSlot { kSfPhi = 60, kSfPsi, kSfF8, kSfFF };
+
 }  // namespace qs
 
 using namespace qs;
@@ -596,6 +624,54 @@ int qexstag_hisq_deriv(qexstag_smear *s, const qexstag_hisq_coefs *c, const doub
   if ((rc = hisq_deriv_dev(s, *c, u, cf, fs, cl, fs, d)) || (rc = smear_out_finish(s, d, deriv, mem))) return rc;
   QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
+}
+
+int qexstag_hisq_force(qexstag_links *g, qexstag_smear *s, const qexstag_hisq_coefs *c, const double *thin,
+                       double *f, const double *phi, double m, const qexstag_solver_params *p,
+                       qexstag_solver_stats *st, int mem) {
+  int rc;
+  if ((rc = check_smear(s, mem))) return rc;
+  if (!g || !g->u64 || !c || !thin || !f || !phi || !p) return fail(QEXSTAG_ERR_ARG, "hisq_force: null argument");
+  if (g->nl != 8) return fail(QEXSTAG_ERR_ARG, "hisq_force: the link handle must hold 8 (fat+Naik) links");
+  if (g->l != s->l) return fail(QEXSTAG_ERR_ARG, "hisq_force: handles on different layouts");
+  if (!finite_coefs(c->fat7first) || !finite_coefs(c->fat7second) || !std::isfinite(c->naik))
+    return fail(QEXSTAG_ERR_ARG, "hisq_force: coefficients not finite");
+  const Geom &geo = s->l->g;
+  const size_t fs = (size_t)9 * geo.V;
+  const size_t vb = sizeof(double2) * 3 * (size_t)geo.V;
+  const double2 *u, *dphi;
+  double2 *df;
+  void *ppsi, *pf8, *pff;
+  if ((rc = smear_in(s, kSmIn0, thin, mem, &u)) || (rc = smear_out_buf(s, kSmOut0, f, mem, &df)) ||
+      (rc = s->ws.get(kSfPsi, vb, &ppsi)) || (rc = s->ws.get(kSfF8, 2 * field4_bytes(geo), &pf8)) ||
+      (rc = s->ws.get(kSfFF, field4_bytes(geo), &pff)))
+    return rc;
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    dphi = (const double2 *)phi;
+  } else {
+    void *soa, *aos;
+    if ((rc = s->ws.get(kSfPhi, vb, &soa)) || (rc = s->ws.get(kSmAos, field4_bytes(geo) / 4, &aos))) return rc;
+    QS_CUDA(cudaMemcpyAsync(aos, phi, vb, cudaMemcpyHostToDevice, stream()));
+    if ((rc = aos_to_soa((const double *)aos, (double2 *)soa, geo.V, geo.V, 3))) return rc;
+    dphi = (const double2 *)soa;
+  }
+  // smear the thin links into the operator (smearGetForce's forward part)
+  if ((rc = hisq_dev(s, *c, u, g->u64, 2 * fs, g->u64 + fs, 2 * fs))) return rc;
+  free_low_links(g->low);
+  if ((rc = build_low_links(g))) return rc;
+  // stagForceSolve, then fermForce's outer products f1 (fat) and f3 (long)
+  double2 *psi = (double2 *)ppsi, *f8 = (double2 *)pf8, *ff = (double2 *)pff;
+  const int status = qexstag_force_solve(g, (double *)psi, (const double *)dphi, m, p, st, QEXSTAG_MEM_DEVICE);
+  if (status < 0) return status;
+  if ((rc = qexstag_ferm_outer(g, (double *)f8, (const double *)psi, QEXSTAG_MEM_DEVICE))) return rc;
+  // u.deriv(ff, f1, f3), then projectTAH(ff U^dag)
+  if ((rc = hisq_deriv_dev(s, *c, u, f8, 2 * fs, f8 + fs, 2 * fs, ff))) return rc;
+  tah_times_adj_kernel<<<field_grid(geo), kSmBlock, 0, stream()>>>(geo.V, ff, u, df, fs);
+  note_launch();
+  QS_LAUNCH_CHECK();
+  if ((rc = smear_out_finish(s, df, f, mem))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return status;
 }
 
 }  // extern "C"

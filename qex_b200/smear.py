@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib as L
-from .stag import Layout, Staggered, _is_torch, _mem_of, _ptr
+from .stag import Layout, SolverParams, Staggered, _is_torch, _mem_of, _ptr
 
 
 @dataclass
@@ -147,6 +147,21 @@ class Smear:
         cc = coef.c()
         L.check(self._lib.qexstag_hisq_deriv(self.handle, C.byref(cc), _ptr(g)[0], _ptr(cfat)[0], _ptr(clong)[0],
                                              _ptr(deriv, True)[0], mem), "hisq_deriv")
+
+    def force(self, stag: Staggered, coef: HisqCoefs, thin, f, phi, m: float, sp: SolverParams) -> None:
+        """QEX's force with HISQ smearing (hmcAction.nim:851-885): f =
+        projectTAH(ff U^dag) on the thin links, ff the chain rule of the
+        fermion force's outer products; stag's links become the smeared ones."""
+        _check_gauge(self.l, thin)
+        _check_gauge(self.l, f)
+        mem = _mem_of(thin, f, phi)
+        st = L.SolverStatsC()
+        pc = sp.c_params()
+        cc = coef.c()
+        rc = self._lib.qexstag_hisq_force(stag.handle, self.handle, C.byref(cc), _ptr(thin)[0], _ptr(f, True)[0],
+                                          _ptr(phi)[0], float(m), C.byref(pc), C.byref(st), mem)
+        L.check(rc, "hisq_force")
+        sp.take(st, rc)
 
     def smear_into(self, stag: Staggered, coef: HisqCoefs, g) -> None:
         """Smear thin links g into a fat+Naik operator's link list and rebuild

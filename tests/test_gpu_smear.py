@@ -199,3 +199,89 @@ def test_hisq_deriv_matches_oracle(cuda, dims, case):
         dd = torch.empty_like(S.to_device_links(g))
         sm.smearDeriv(coef, S.to_device_links(g), S.to_device_links(cf), S.to_device_links(cl), dd)
         assert np.array_equal(S.to_host_links(dd), d)
+
+
+# ---- HISQ fermion force ------------------------------------------------------
+
+def oracle_hisq_force(dims, thin, phi, m):
+    """QEX's force with HISQ smearing, composed from the oracle's pieces."""
+    fl, ll = O.hisq_smear(dims, thin)
+    o = O.Oracle(dims, F.interleave(fl, ll))
+    psi = o.vec()
+    o.force_solve(psi, phi, m, 1e-26)
+    f8 = np.zeros((8,) + thin.shape[1:], complex)
+    o.ferm_outer(f8, psi)
+    ff = O.hisq_deriv(dims, thin, f8[0::2], f8[1::2])
+    m = (ff @ np.conj(np.swapaxes(thin, -1, -2))).reshape(-1, 3, 3)
+    return np.stack([O.project_tah(x) for x in m]).reshape(thin.shape)
+
+
+def test_hisq_force_matches_oracle(cuda):
+    dims = (4, 6, 4, 8)
+    V = F.volume(dims)
+    lay = S.Layout(dims)
+    thin_links = thin(dims, 12, 0.4)
+    phi = F.gaussian_vector(V, 13)
+    phi[V // 2:] = 0
+    stag = S.Staggered(lay, np.zeros((8, V, 3, 3), complex) + np.eye(3))
+    sm = SM.Smear(lay)
+    f = np.empty_like(thin_links)
+    sp = S.SolverParams(r2req=1e-26)
+    sm.force(stag, SM.newHISQ(), thin_links, f, phi, 0.2, sp)
+    fo = oracle_hisq_force(dims, thin_links, phi, 0.2)
+    assert rel(f, fo) < 1e-10
+    # the operator now holds the smeared links
+    ofl, oll = O.hisq_smear(dims, thin_links)
+    o = O.Oracle(dims, F.interleave(ofl, oll))
+    x = F.gaussian_vector(V, 14)
+    a, b = np.zeros_like(x), np.zeros_like(x)
+    stag.D(a, x, 0.2)
+    o.D(b, x, 0.2)
+    assert rel(a, b) < TOL
+
+
+def test_hisq_force_finite_differences(cuda):
+    """S = phi_e^dag A^-1 phi_e, A = stagD2ee(m^2) of the HISQ-smeared thin
+    links; along W -> exp(t T_a) W on one thin link, dS/dt = Re Tr[T_a
+    f^dag]/8 (f carries QEX's factor 4 in psi and S_QEX = 2 S)."""
+    torch = cuda
+    from qex_b200.force_check import gell_mann
+    dims = (4, 4, 4, 6)
+    V = F.volume(dims)
+    h = V // 2
+    m = 0.2
+    lay = S.Layout(dims)
+    g = thin(dims, 15, 0.4)
+    phi = F.gaussian_vector(V, 16)
+    phi[h:] = 0
+    stag = S.Staggered(lay, np.zeros((8, V, 3, 3), complex) + np.eye(3))
+    sm = SM.Smear(lay)
+    coef = SM.newHISQ()
+    f = np.empty_like(g)
+    sm.force(stag, coef, g, f, phi, m, S.SolverParams(r2req=1e-26))
+    T = gell_mann()
+    rng = np.random.default_rng(17)
+    eps = 1e-5
+    worst, scale = 0.0, 0.0
+    for _ in range(6):
+        mu, x = int(rng.integers(0, 4)), int(rng.integers(0, V))
+        for a in (0, 3, 7):
+            ys, gs = [], []
+            for e in (eps, -eps):
+                gp = g.copy()
+                gp[mu, x] = F.exp_ah(T[a][None], e)[0] @ g[mu, x]
+                gs.append(gp)
+                sm.smear_into(stag, coef, gp)
+                y = np.zeros_like(phi)
+                stag.solveEE(y, phi, m, S.SolverParams(r2req=1e-26))
+                ys.append(y)
+            am, ap = np.zeros_like(phi), np.zeros_like(phi)
+            sm.smear_into(stag, coef, gs[1])
+            stag.stagD2ee(am, ys[1], m * m)
+            sm.smear_into(stag, coef, gs[0])
+            stag.stagD2ee(ap, ys[1], m * m)
+            fd = np.vdot(ys[0][:h], (am - ap)[:h]).real / (2 * eps)
+            an = np.trace(T[a] @ np.conj(f[mu, x]).T).real / 8
+            worst = max(worst, abs(fd - an))
+            scale = max(scale, abs(an))
+    assert worst < 1e-6 * scale
