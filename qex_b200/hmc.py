@@ -132,7 +132,7 @@ class StaggeredFermion:
     naik = None gives the naive operator (fat only)."""
 
     def __init__(self, lat: Lattice, mass: float, naik: float | None = -1.0 / 24.0,
-                 r2req_action=1e-20, r2req_force=1e-18, sloppy=S.L.SLOPPY_HALF):
+                 r2req_action=1e-20, r2req_force=1e-18, sloppy=S.L.SLOPPY_HALF, hisq: bool = False):
         self.lat = lat
         self.mass = mass
         self.naik = naik
@@ -141,6 +141,15 @@ class StaggeredFermion:
         self.phi = None
         self.r2a, self.r2f, self.sloppy = r2req_action, r2req_force, sloppy
         self.solver_iterations = 0
+        # HISQ: the operator's fat and long links are the library's HISQ
+        # smearing of the phased thin links (hmcAction.nim:540-555), and the
+        # force is its qexstag_hisq_force (smearing chain rule included)
+        self.hisq = hisq
+        if hisq:
+            from . import smear as SM
+            self.sm = SM.Smear(self.lay)
+            self.coef = SM.newHISQ()
+            self.smear_seconds = 0.0
 
     def links(self, U):
         lat = self.lat
@@ -154,7 +163,17 @@ class StaggeredFermion:
         g[1::2] = lng
         return g
 
+    def phased_thin(self, U):
+        return (U * self.lat.sign1[:, :, None, None]).permute(0, 2, 3, 1).contiguous()
+
     def set_links(self, U):
+        if self.hisq:
+            if self.stag is None:
+                eye = torch.eye(3, dtype=U.dtype, device=U.device)
+                init = eye.reshape(1, 3, 3, 1).expand(8, 3, 3, self.lat.V).contiguous()
+                self.stag = S.Staggered(self.lay, init, long_coeff=self.coef.naik)
+            self.sm.smear_into(self.stag, self.coef, self.phased_thin(U))
+            return
         dev = self.links(U).permute(0, 2, 3, 1).contiguous()
         if self.stag is None:
             self.stag = S.Staggered(self.lay, dev, long_coeff=self.naik if self.naik else 1.0)
@@ -196,6 +215,15 @@ class StaggeredFermion:
         """F = TAH(G) with dS_F/deps = Re Tr[T G^dagger]; S_F = 0.5|D(-m)^-1 phi|^2
         changes by Re Tr[dW f^dagger]/4 for a change dW of a phased link W."""
         lat = self.lat
+        if self.hisq:
+            if self.stag is None:
+                self.set_links(U)
+            f = torch.empty((4, 3, 3, lat.V), dtype=torch.complex128, device="cuda")
+            sp = S.SolverParams(r2req=self.r2f, sloppySolve=self.sloppy)
+            self.sm.force(self.stag, self.coef, self.phased_thin(U), f, self.phi, self.mass, sp)
+            self.solver_iterations += sp.iterations
+            # the generator acting on W = eta U acts on U the same way
+            return 0.25 * f.permute(0, 3, 1, 2)
         f = self.outer(U)
         nl = f.shape[0]
         out = []
@@ -258,13 +286,13 @@ def random_momenta(lat: Lattice, gen: np.random.Generator):
 
 
 def trajectory_with_reversal(lat, U0, beta, mass, naik, tau, nsteps, seed=7, sloppy=S.L.SLOPPY_HALF,
-                             r2req_action=1e-20, r2req_force=1e-20):
+                             r2req_action=1e-20, r2req_force=1e-20, hisq=False):
     """One trajectory from (U0, p0) and its reversal (flip p, evolve back).
     Returns a dict with H values, dH, and the reversibility errors."""
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
     ferm = StaggeredFermion(lat, mass, naik, r2req_action=r2req_action, r2req_force=r2req_force,
-                            sloppy=sloppy)
+                            sloppy=sloppy, hisq=hisq)
     ferm.heatbath(U0, gen)
     hmc = HMC(lat, beta, ferm)
     p0 = random_momenta(lat, np.random.default_rng(seed))
@@ -309,6 +337,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--tau", type=float, default=1.0)
     ap.add_argument("--naive", action="store_true")
+    ap.add_argument("--hisq", action="store_true", help="HISQ-smeared fermion operator and force")
     ap.add_argument("--therm", type=int, default=10)
     a = ap.parse_args()
     dims = tuple(int(v) for v in a.dims.split(","))
@@ -319,7 +348,9 @@ def main():
     t0 = time.perf_counter()
     U0, acc = thermalize(lat, U0, a.beta, a.therm)
     t1 = time.perf_counter()
-    out = trajectory_with_reversal(lat, U0, a.beta, a.mass, None if a.naive else -1.0 / 24.0, a.tau, a.steps)
+    out = trajectory_with_reversal(lat, U0, a.beta, a.mass, None if a.naive else -1.0 / 24.0, a.tau, a.steps,
+                                   hisq=a.hisq)
+    out["fermion"] = "hisq" if a.hisq else ("naive" if a.naive else "thin fat+Naik")
     out["seconds"] = time.perf_counter() - t1
     out["thermalization"] = {"trajectories": a.therm, "accepted": acc, "seconds": t1 - t0}
     out["plaquette"] = -out.pop("plaquette_action") / (a.beta / 3.0) / (6 * lat.V * 3)

@@ -139,3 +139,50 @@ def test_hmc_force_matches_finite_difference(cuda):
         fd = (vals[0] - vals[1]) / (2 * eps)
         an = torch.trace(T @ hmc.dagger(Fo[mu, x])).real.item()
         assert abs(fd - an) <= 1e-5 * max(abs(an), 1.0), (mu, x, fd, an)
+
+
+def test_hisq_hmc_force_matches_finite_difference(cuda):
+    """HISQ molecular-dynamics force: Wilson plus the pseudofermion of the
+    HISQ-smeared operator (qexstag_hisq_force: smearing chain rule through
+    fat7, projectU, fat7 + Naik) against a central difference of the
+    potential along su(3) generators on the thin links."""
+    torch = cuda
+    from qex_b200 import hmc
+    dims = (4, 4, 4, 8)
+    lat = hmc.Lattice(dims)
+    U = torch.from_numpy(F.gauge_warm(dims, 0.3, 6)).to("cuda")
+    ferm = hmc.StaggeredFermion(lat, 0.2, r2req_action=1e-26, r2req_force=1e-26, sloppy=S.L.SLOPPY_NONE,
+                                hisq=True)
+    ferm.heatbath(U, torch.Generator(device="cuda").manual_seed(3))
+    h = hmc.HMC(lat, 5.6, ferm)
+    Fo = h.force(U)
+    rng = np.random.default_rng(4)
+    eps = 1e-5
+    for _ in range(6):
+        mu, x = int(rng.integers(0, 4)), int(rng.integers(0, lat.V))
+        T = torch.from_numpy(F.rand_tah(1, rng)[0]).to("cuda")
+        vals = []
+        for e in (eps, -eps):
+            Up = U.clone()
+            Up[mu, x] = hmc.exp_ah(e * T) @ U[mu, x]
+            vals.append(h.potential(Up))
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        an = torch.trace(T @ hmc.dagger(Fo[mu, x])).real.item()
+        assert abs(fd - an) <= 1e-5 * max(abs(an), 1.0), (mu, x, fd, an)
+
+
+def test_hisq_hmc_trajectory_reversible(cuda):
+    """HISQ trajectories (QEX's tgenerichmchisq shape): dH falls as the square
+    of the step and the reversed trajectory returns to the start."""
+    torch = cuda
+    from qex_b200 import hmc
+    dims = (8, 8, 8, 8)
+    lat = hmc.Lattice(dims)
+    U0 = torch.from_numpy(F.gauge_warm(dims, 0.3, 43)).to("cuda")
+    outs = [hmc.trajectory_with_reversal(lat, U0, 5.6, 0.1, None, 0.5, n, sloppy=S.L.SLOPPY_NONE,
+                                         r2req_action=1e-24, r2req_force=1e-24, hisq=True) for n in (10, 20)]
+    ratio = outs[0]["dH"] / outs[1]["dH"]
+    assert 3.0 < ratio < 5.0, (ratio, outs)
+    for out in outs:
+        assert out["max_dU"] < 1e-7 and out["max_dp"] < 1e-7, out
+        assert abs(out["dH_reversed"]) < 1e-5, out
