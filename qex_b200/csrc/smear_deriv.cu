@@ -10,7 +10,7 @@
 // forward sweep (smear.cu).  With M the chain on the fat links:
 //   sweep A: T7[mu][sig] = St(U_sig; M_mu)        (chain of the 7-staples on
 //            the 5-staples, up to c7: M5[mu][nu][rho] = c5 M_mu + c7 T7[mu][sig])
-//   sweep B: M3[mu][nu] = c3 M_mu + cL St(U_nu; M_mu) + sum_rho St(U_rho; M5)
+//   sweep B: M3[mu][nu] = c3 M_mu + cL T7[mu][nu] + sum_rho St(U_rho; M5)
 //            (chain on the 3-staples)
 //   sweep C: dU_d(y) = c1' M_d + sum_nu St(U_nu; M3[d][nu])   (U_d as the
 //            middle link of its 3-staples) + the derivatives of every staple
@@ -42,27 +42,28 @@ __device__ __forceinline__ void m_nd(M3 &r, const M3 &a, const M3 &b) {
     }
 }
 
-// a field operand a*A + b*B (B may be absent), element e of site s at e*V + s
-struct Lin2 {
-  const double2 *a, *b;
-  double ca, cb;
+// a field operand sum_k c_k F_k of N fields, element e of site s at e*V + s;
+// terms with a zero coefficient are skipped (their pointer may be null)
+template <int N>
+struct Lin {
+  const double2 *p[N];
+  double c[N];
   __device__ __forceinline__ double2 ld(size_t o) const {
-    const double2 x = __ldg(a + o);
-    double2 r = make_double2(ca * x.x, ca * x.y);
-    if (b) {
-      const double2 y = __ldg(b + o);
-      r.x = fma(cb, y.x, r.x);
-      r.y = fma(cb, y.y, r.y);
-    }
+    double2 r = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < N; k++)
+      if (c[k] != 0.0) {
+        const double2 x = __ldg(p[k] + o);
+        r.x = fma(c[k], x.x, r.x);
+        r.y = fma(c[k], x.y, r.y);
+      }
     return r;
   }
 };
-__device__ __forceinline__ Lin2 lin(const double2 *a, double ca = 1.0, const double2 *b = nullptr, double cb = 0.0) {
-  Lin2 l;
-  l.a = a;
-  l.b = b;
-  l.ca = ca;
-  l.cb = cb;
+__device__ __forceinline__ Lin<1> lin(const double2 *a, double ca = 1.0) {
+  Lin<1> l;
+  l.p[0] = a;
+  l.c[0] = ca;
   return l;
 }
 
@@ -137,10 +138,11 @@ __device__ __forceinline__ void acc_dn_nn(M3 &acc, double coef, const FA &A, int
 }
 
 // acc += coef St(g; F) for link direction mu, staple direction nu
+template <class FF>
 __device__ __forceinline__ void staple_acc(M3 &acc, double coef, const Geom &g, const SiteCtx &c, int mu, int nu,
-                                           const double2 *Un, const Lin2 &F) {
+                                           const double2 *Un, const FF &F) {
   const size_t V = (size_t)g.V;
-  const Lin2 U = lin(Un);
+  const Lin<1> U = lin(Un);
   const int s_pn = disp1(g, c.x, c.lex, c.par, nu, 1);
   const int s_pm = disp1(g, c.x, c.lex, c.par, mu, 1);
   const int s_mn = disp1(g, c.x, c.lex, c.par, nu, -1);
@@ -151,10 +153,11 @@ __device__ __forceinline__ void staple_acc(M3 &acc, double coef, const Geom &g, 
 
 // acc += coef d/dg1 [chain c on St(g1; g2)] at y, g1 the side field of this
 // thread's direction d (= d1), g2 of link direction d2
+template <class F2, class FC>
 __device__ __forceinline__ void side_acc(M3 &acc, double coef, const Geom &g, const SiteCtx &c, int d, int d2,
-                                         const double2 *G1, const Lin2 &G2, const Lin2 &C) {
+                                         const double2 *G1, const F2 &G2, const FC &C) {
   const size_t V = (size_t)g.V;
-  const Lin2 g1 = lin(G1);
+  const Lin<1> g1 = lin(G1);
   const int s_p2 = disp1(g, c.x, c.lex, c.par, d2, 1);
   const int s_p1 = disp1(g, c.x, c.lex, c.par, d, 1);
   const int s_m2 = disp1(g, c.x, c.lex, c.par, d2, -1);
@@ -191,18 +194,13 @@ __device__ __forceinline__ int other_index(int mu, int d) { return d < mu ? d : 
 // index r of rho among the two directions other than mu and nu
 __device__ __forceinline__ int third_index(int mu, int nu, int rho) { return rho < 6 - mu - nu - rho ? 0 : 1; }
 
-// chain on the 5-staple S5[mu][nu][rho] (sig the fourth direction)
-__device__ __forceinline__ Lin2 m5_of(const AdjArgs &A, int mu, int sig) {
-  return lin(A.m + mu * A.mfs, A.c5, A.c7 != 0.0 ? A.t7 + fld(A.g, mu * 3 + other_index(mu, sig)) : nullptr, A.c7);
-}
-
 // sweep A: T7[mu][k] = St(U_sig; M_mu), sig = other_dir(mu, k)
 __global__ void __launch_bounds__(kSmBlock, 3) fat7_adj_seven_kernel(const AdjArgs A) {
   SiteCtx c;
   if (!site_of_thread(A.g, c)) return;
   const int mu = c.mu;
   const size_t V = (size_t)A.g.V;
-  const Lin2 M = lin(A.m + mu * A.mfs);
+  const Lin<1> M = lin(A.m + mu * A.mfs);
 #pragma unroll 1
   for (int k = 0; k < 3; k++) {
     const int sig = other_dir(mu, k);
@@ -214,7 +212,9 @@ __global__ void __launch_bounds__(kSmBlock, 3) fat7_adj_seven_kernel(const AdjAr
   }
 }
 
-// sweep B: M3[mu][j] = c3 M_mu + cL St(U_nu; M_mu) + sum_rho St(U_rho; M5[mu][nu][rho])
+// sweep B: M3[mu][j] = c3 M_mu + cL St(U_nu; M_mu) + sum_rho St(U_rho; M5[mu][nu][rho]).
+// St(U_x; M_mu) is T7[mu][x], so only the c7 part of M5 needs new staples:
+//   M3 = c3 M + cL T7[mu][nu] + sum_rho (c5 T7[mu][rho] + c7 St(U_rho; T7[mu][sig]))
 __global__ void __launch_bounds__(kSmBlock, 3) fat7_adj_three_kernel(const AdjArgs A) {
   SiteCtx c;
   if (!site_of_thread(A.g, c)) return;
@@ -224,16 +224,24 @@ __global__ void __launch_bounds__(kSmBlock, 3) fat7_adj_three_kernel(const AdjAr
 #pragma unroll 1
   for (int j = 0; j < 3; j++) {
     const int nu = other_dir(mu, j);
-    M3 S;
+    M3 S, t;
     m_load(S, Mm, V, c.site);
     m_scale(S, A.c3);
-    if (A.cl != 0.0) staple_acc(S, A.cl, A.g, c, mu, nu, A.u + nu * A.ufs, lin(Mm));
+    if (A.cl != 0.0) {
+      m_load(t, A.t7 + fld(A.g, mu * 3 + j), V, c.site);
+      m_axpy(S, A.cl, t);
+    }
     if (A.do5) {
 #pragma unroll 1
       for (int r = 0; r < 2; r++) {
         const int rho = third_dir(mu, nu, r);
         const int sig = 6 - mu - nu - rho;
-        staple_acc(S, 1.0, A.g, c, mu, rho, A.u + rho * A.ufs, m5_of(A, mu, sig));
+        if (A.c5 != 0.0) {
+          m_load(t, A.t7 + fld(A.g, mu * 3 + other_index(mu, rho)), V, c.site);
+          m_axpy(S, A.c5, t);
+        }
+        if (A.c7 != 0.0)
+          staple_acc(S, A.c7, A.g, c, mu, rho, A.u + rho * A.ufs, lin(A.t7 + fld(A.g, mu * 3 + other_index(mu, sig))));
       }
     }
     m_store(A.m3 + fld(A.g, mu * 3 + j), V, c.site, S);
@@ -267,7 +275,10 @@ __global__ void __launch_bounds__(kSmBlock, 3) fat7_adj_link_kernel(const AdjArg
       const int nu = other_dir(d, j);
       staple_acc(acc, 1.0, g, c, d, nu, A.u + nu * A.ufs, lin(A.m3 + fld(g, d * 3 + j)));
     }
-    // U_d as a side link
+    // U_d as a side link.  A side derivative is linear in its middle field
+    // and in its chain, so the terms with chain M_mu are taken together:
+    // Lepage (cL, middle S3[mu][d]), the c5 part of the 5-staples (middle
+    // S3[mu][nu]) and the 7-staples (c7, middle S5[mu][nu][rho]).
 #pragma unroll 1
     for (int jm = 0; jm < 3; jm++) {
       const int mu = other_dir(d, jm);
@@ -275,20 +286,28 @@ __global__ void __launch_bounds__(kSmBlock, 3) fat7_adj_link_kernel(const AdjArg
       const double2 *Mm = A.m + mu * A.mfs;
       // 3-staple S3[mu][d] = St(U_d; U_mu), chain M3[mu][d]
       side_acc(acc, 1.0, g, c, d, mu, Ud, lin(A.u + mu * A.ufs), lin(A.m3 + fld(g, mu * 3 + jd)));
-      // Lepage staple St(U_d; S3[mu][d]), chain cL M_mu
-      if (A.cl != 0.0) side_acc(acc, A.cl, g, c, d, mu, Ud, lin(A.s3 + fld(g, mu * 3 + jd)), lin(Mm));
-      if (A.do5) {
-#pragma unroll 1
-        for (int r = 0; r < 2; r++) {
-          const int nu = third_dir(mu, d, r);
-          const int jn = other_index(mu, nu);
-          const int rho = 6 - mu - nu - d;  // the fourth direction
-          // 5-staple S5[mu][nu][d] = St(U_d; S3[mu][nu]), chain M5[mu][nu][d] (sig = rho)
-          side_acc(acc, 1.0, g, c, d, mu, Ud, lin(A.s3 + fld(g, mu * 3 + jn)), m5_of(A, mu, rho));
-          // 7-staple St(U_d; S5[mu][nu][rho]), chain c7 M_mu
-          if (A.c7 != 0.0)
-            side_acc(acc, A.c7, g, c, d, mu, Ud, lin(A.s5 + fld(g, (mu * 3 + jn) * 2 + third_index(mu, nu, rho))),
-                     lin(Mm));
+      if (A.have5) {
+        const int nu0 = third_dir(mu, d, 0), nu1 = third_dir(mu, d, 1);
+        const int jn0 = other_index(mu, nu0), jn1 = other_index(mu, nu1);
+        const int rho0 = 6 - mu - nu0 - d, rho1 = 6 - mu - nu1 - d;  // the fourth directions
+        Lin<5> G;
+        G.p[0] = A.s3 + fld(g, mu * 3 + jd);
+        G.c[0] = A.cl;
+        G.p[1] = A.s3 + fld(g, mu * 3 + jn0);
+        G.c[1] = A.c5;
+        G.p[2] = A.s3 + fld(g, mu * 3 + jn1);
+        G.c[2] = A.c5;
+        G.p[3] = A.c7 != 0.0 ? A.s5 + fld(g, (mu * 3 + jn0) * 2 + third_index(mu, nu0, rho0)) : nullptr;
+        G.c[3] = A.c7;
+        G.p[4] = A.c7 != 0.0 ? A.s5 + fld(g, (mu * 3 + jn1) * 2 + third_index(mu, nu1, rho1)) : nullptr;
+        G.c[4] = A.c7;
+        side_acc(acc, 1.0, g, c, d, mu, Ud, G, lin(Mm));
+        // the c7 part of the 5-staple chains M5[mu][nu][d] = c5 M_mu + c7 T7[mu][rho]
+        if (A.c7 != 0.0) {
+          side_acc(acc, A.c7, g, c, d, mu, Ud, lin(A.s3 + fld(g, mu * 3 + jn0)),
+                   lin(A.t7 + fld(g, mu * 3 + other_index(mu, rho0))));
+          side_acc(acc, A.c7, g, c, d, mu, Ud, lin(A.s3 + fld(g, mu * 3 + jn1)),
+                   lin(A.t7 + fld(g, mu * 3 + other_index(mu, rho1))));
         }
       }
     }
@@ -450,7 +469,7 @@ int fat7_adj_dev(const Geom &g, const qexstag_fat7_coefs &c, const double2 *u, s
   A.have3 = (c.three_staple != 0.0 || A.have5) ? 1 : 0;
   A.do5 = (c.five_staple != 0.0 || c.seven_staple != 0.0) ? 1 : 0;
   const dim3 grid = sweep_grid(g);
-  if (A.c7 != 0.0) {
+  if (A.have5) {
     fat7_adj_seven_kernel<<<grid, kSmBlock, 0, stream()>>>(A);
     note_launch();
   }

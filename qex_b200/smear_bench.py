@@ -31,6 +31,12 @@ FAT7_FULL = 4 * LINK * (1 + 3 + 1) + 4 * LINK * (1 + 3 + 1 + 6 + 1) + 4 * LINK *
 PROJECT = 2 * 4 * LINK
 NAIK = 2 * 4 * LINK
 QEX_FLOPS_FAT7 = 61632
+# adjoint of one fat7 level: sweep A reads M and U, writes 12 T7 fields;
+# sweep B reads M, U, T7, writes 12 M3 fields; sweep C reads M, U, M3, T7,
+# the 12 S3 and 24 S5 forward fields and writes the derivative
+ADJ_FULL = 4 * LINK * (2 + 3) + 4 * LINK * (2 + 3 + 3) + 4 * LINK * (2 + 3 + 3 + 3 + 6 + 1)
+ADJ_NAIK = 4 * LINK  # the long-link chain, read once more by sweep C
+PROJECT_DERIV = 4 * LINK * 4  # reads v, w, the chain; writes the result
 
 
 def timed(fn, reps):
@@ -71,6 +77,17 @@ def run(dims, reps):
     stage("fat7_second_naik", lambda: sm.makeImpLinks(fl, w, coef.fat7second, ll, w, coef.naik),
           FAT7_FULL + NAIK, QEX_FLOPS_FAT7)
     stage("hisq_smear", lambda: sm.smear(coef, g, fl, ll), 2 * FAT7_FULL + PROJECT + NAIK, 2 * QEX_FLOPS_FAT7)
+    # chain rule (smearGetForce's smearedForce) for Gaussian chains on the fat
+    # and long links: forward smear with the second level's staples, the
+    # second level's adjoint (+ Naik), projectU's, the first level's staples
+    # again and its adjoint
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    cf = torch.complex(torch.randn(g.shape, dtype=torch.float64, device="cuda", generator=gen),
+                       torch.randn(g.shape, dtype=torch.float64, device="cuda", generator=gen))
+    cl = cf.flip(0).contiguous()
+    d = torch.empty_like(g)
+    deriv_bytes = 3 * FAT7_FULL + PROJECT + 2 * ADJ_FULL + ADJ_NAIK + PROJECT_DERIV
+    stage("hisq_deriv", lambda: sm.smearDeriv(coef, g, cf, cl, d), deriv_bytes, None)
     return out
 
 
