@@ -55,6 +55,7 @@ extern "C" {
 #define QEXSTAG_ERR_TIMEOUT (-4)
 #define QEXSTAG_ERR_ALLOC (-5)
 #define QEXSTAG_ERR_STATE (-6)
+#define QEXSTAG_ERR_IO (-7)     /* gauge file: unreadable, malformed or failed checksum */
 
 /* where field pointers live */
 #define QEXSTAG_MEM_HOST 0
@@ -343,6 +344,45 @@ int qexstag_hisq_deriv(qexstag_smear *s, const qexstag_hisq_coefs *c, const doub
 int qexstag_hisq_force(qexstag_links *g, qexstag_smear *s, const qexstag_hisq_coefs *c, const double *thin,
                        double *f, const double *phi, double m, const qexstag_solver_params *p,
                        qexstag_solver_stats *st, int mem);
+
+/* ---- gauge-field files (QEX's loadGauge / saveGauge,
+   src/gauge/gaugeUtils.nim:96-131, over src/io/readerQiolite.nim and
+   src/io/writerQiolite.nim; MILC files as src/new/milcIO.nim) ----
+   The links are the 4-direction gauge field of qexstag_hisq_smear's
+   convention (double[4][V][3][3][2] host, double2[4][9][V] device), without
+   staggered phases, as QEX holds them between solves. */
+
+#define QEXSTAG_GAUGE_SCIDAC 1  /* USQCD SciDAC single-file LIME (QIO layout), big-endian */
+#define QEXSTAG_GAUGE_ILDG 2    /* ILDG LIME: SciDAC records plus ildg-format / ildg-binary-data */
+#define QEXSTAG_GAUGE_MILC 3    /* MILC binary, version 5 (single precision) */
+
+typedef struct {
+  int format;                  /* QEXSTAG_GAUGE_* */
+  int dims[4];
+  int precision;               /* bytes per real in the file: 4 or 8 */
+  int has_checksum;            /* the file stores a checksum */
+  unsigned file_checksum[2];   /* as stored: SciDAC suma, sumb or MILC sum29, sum31 */
+  unsigned data_checksum[2];   /* of the data read (qexstag_gauge_read only) */
+  char date[64];
+  char file_metadata[256];     /* user XML of the file (truncated) */
+  char record_metadata[256];   /* user XML of the record (truncated) */
+} qexstag_gauge_info;
+
+/* Format, lattice, precision and metadata of a gauge file, without reading
+   the links (getFileLattice, readerQiolite.nim:11-17). */
+int qexstag_gauge_file_info(const char *path, qexstag_gauge_info *info);
+/* Read a SciDAC, ILDG or MILC gauge file into links (reordered to the
+   layout's site index, converted to FP64) and verify its checksum on the
+   GPU.  The file lattice must equal the layout's.  Returns QEXSTAG_ERR_IO
+   on a checksum mismatch, with the links written and both checksums in
+   info (which may be NULL). */
+int qexstag_gauge_read(qexstag_layout *l, const char *path, double *links, int mem, qexstag_gauge_info *info);
+/* Write links as a SciDAC or ILDG file (precision 4 or 8 bytes, with the
+   scidac-checksum record) or a MILC file (precision 4, this machine's byte
+   order); file_md and record_md are the user XML of the file and the
+   record (may be NULL). */
+int qexstag_gauge_write(qexstag_layout *l, const char *path, const double *links, int mem, int format,
+                        int precision, const char *file_md, const char *record_md);
 
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */

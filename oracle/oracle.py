@@ -22,7 +22,7 @@ _lib = None
 
 
 def build() -> Path:
-    srcs = [HERE / "qexstag_oracle.c", HERE / "smear_oracle.c"]
+    srcs = [HERE / "qexstag_oracle.c", HERE / "smear_oracle.c", HERE / "io_oracle.c"]
     if not LIB.exists() or any(LIB.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB
@@ -72,6 +72,9 @@ def lib():
             "or_project_u_deriv": (None, [C.c_long, P, P, P, P, D]),
             "or_sylsolve": (None, [C.c_long, P, P, P]),
             "or_hisq_deriv": (None, [C.POINTER(C.c_int), DP, DP, D, D, P, P, P, P]),
+            "or_crc32": (C.c_uint32, [P, C.c_size_t]),
+            "or_scidac_checksum": (None, [P, C.c_long, C.c_long, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+            "or_milc_checksum": (None, [P, C.c_long, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(l, name)

@@ -19,6 +19,8 @@ ERR_NAN = -3
 ERR_TIMEOUT = -4
 ERR_ALLOC = -5
 ERR_STATE = -6
+ERR_IO = -7
+GAUGE_SCIDAC, GAUGE_ILDG, GAUGE_MILC = 1, 2, 3
 
 MEM_HOST = 0
 MEM_DEVICE = 1
@@ -61,6 +63,20 @@ class HisqCoefsC(C.Structure):
         ("fat7second", Fat7CoefsC),
         ("naik", C.c_double),
         ("reunit_eps", C.c_double),
+    ]
+
+
+class GaugeInfoC(C.Structure):
+    _fields_ = [
+        ("format", C.c_int),
+        ("dims", C.c_int * 4),
+        ("precision", C.c_int),
+        ("has_checksum", C.c_int),
+        ("file_checksum", C.c_uint * 2),
+        ("data_checksum", C.c_uint * 2),
+        ("date", C.c_char * 64),
+        ("file_metadata", C.c_char * 256),
+        ("record_metadata", C.c_char * 256),
     ]
 
 
@@ -116,6 +132,9 @@ SIGNATURES = {
     "qexstag_project_u_deriv": (I, [P, P, P, P, P, D, I]),
     "qexstag_hisq_deriv": (I, [P, P, P, P, P, P, I]),
     "qexstag_hisq_force": (I, [P, P, P, P, P, P, D, P, P, I]),
+    "qexstag_gauge_file_info": (I, [C.c_char_p, P]),
+    "qexstag_gauge_read": (I, [P, C.c_char_p, P, I, P]),
+    "qexstag_gauge_write": (I, [P, C.c_char_p, P, I, I, I, C.c_char_p, C.c_char_p]),
 }
 
 _lib = None
