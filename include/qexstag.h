@@ -384,6 +384,44 @@ int qexstag_gauge_read(qexstag_layout *l, const char *path, double *links, int m
 int qexstag_gauge_write(qexstag_layout *l, const char *path, const double *links, int mem, int format,
                         int precision, const char *file_md, const char *record_md);
 
+/* ---- gauge action, gauge force and the molecular-dynamics updates
+   (src/gauge/gaugeAction.nim, src/gauge/gaugeUtils.nim:419-459, 1466-1493,
+   src/hmc/hmcAction.nim:248-304) ----
+   Link fields and momenta are 4-direction fields as for
+   qexstag_hisq_smear (host double[4][V][3][3][2], device double2[4][9][V]);
+   the gauge links carry no staggered phases. */
+
+/* GaugeActionCoeffs (gaugeAction.nim:14-19), plaquette and rectangle terms */
+typedef struct {
+  double plaq, rect;
+} qexstag_gauge_coefs;
+/* gaugeActRect (gaugeAction.nim:51-53): plaq = (1 - 8 c1) beta, rect = c1
+   beta; c1 = -1/12 is tree-level Symanzik, -0.331 Iwasaki, -1.4088 DBW2,
+   0 Wilson. */
+void qexstag_gauge_coefs_rect(qexstag_gauge_coefs *c, double beta, double c1);
+/* gaugeAction1 (gaugeAction.nim:487-571): -(1/3) (plaq sum_{x,mu>nu} Re Tr
+   P_munu(x) + rect sum_{x,mu!=nu} Re Tr R_munu(x)). */
+int qexstag_gauge_action(qexstag_layout *l, const qexstag_gauge_coefs *c, const double *u, int mem,
+                         double *action);
+/* gaugeForce (gaugeAction.nim:576-779): f_mu(x) = projectTAH(U_mu(x) C_mu(x)),
+   C the plaq/3- and rect/3-weighted sums of the paths that close each
+   plaquette and rectangle through U_mu(x); along U -> exp(t T) U the action
+   changes at rate Re Tr[T^dag f]. */
+int qexstag_gauge_force(qexstag_layout *l, const qexstag_gauge_coefs *c, const double *u, double *f, int mem);
+/* axexpmuly(u, eps, p, u) (gaugeUtils.nim:452-459): u <- expAH(eps p) u with
+   QEX's expAH (scaling, degree-12 Taylor, squaring; matexp.nim:316-346). */
+int qexstag_link_update(qexstag_layout *l, double *u, const double *p, double eps, int mem);
+/* p <- p + a f (mdv's p -= f with a = -1, hmcAction.nim:288-296). */
+int qexstag_momenta_update(qexstag_layout *l, double *p, const double *f, double a, int mem);
+/* p = randomTAH (randTah3, gaugeUtils.nim:1466-1493): Gaussian su(3)
+   momenta from a counter-based generator (Philox-4x32-10), link k of the
+   field drawing from (k, counter) under key seed, so a (seed, counter) pair
+   reproduces the field on any device. */
+int qexstag_momenta_heatbath(qexstag_layout *l, double *p, unsigned long long seed, unsigned long long counter,
+                             int mem);
+/* kineticAction (hmcAction.nim:248-255): 0.5 sum |p|^2 - 16 V. */
+int qexstag_kinetic_action(qexstag_layout *l, const double *p, int mem, double *t);
+
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */
 

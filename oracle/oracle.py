@@ -22,7 +22,7 @@ _lib = None
 
 
 def build() -> Path:
-    srcs = [HERE / "qexstag_oracle.c", HERE / "smear_oracle.c", HERE / "io_oracle.c"]
+    srcs = [HERE / "qexstag_oracle.c", HERE / "smear_oracle.c", HERE / "io_oracle.c", HERE / "hmc_oracle.c"]
     if not LIB.exists() or any(LIB.stat().st_mtime < s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-C", str(HERE)], check=True, capture_output=True)
     return LIB
@@ -73,6 +73,10 @@ def lib():
             "or_sylsolve": (None, [C.c_long, P, P, P]),
             "or_hisq_deriv": (None, [C.POINTER(C.c_int), DP, DP, D, D, P, P, P, P]),
             "or_crc32": (C.c_uint32, [P, C.c_size_t]),
+            "or_gauge_action": (D, [C.POINTER(C.c_int), D, D, P]),
+            "or_gauge_force": (None, [C.POINTER(C.c_int), D, D, P, P]),
+            "or_exp_ah": (None, [C.c_long, P, D, P]),
+            "or_link_update": (None, [C.c_long, P, P, D]),
             "or_scidac_checksum": (None, [P, C.c_long, C.c_long, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
             "or_milc_checksum": (None, [P, C.c_long, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
         }
@@ -304,3 +308,36 @@ def hisq_deriv(dims, g, cfat, clong, lepage: float = 0.0, naik: float = 1.0, eps
     d = np.empty_like(g)
     lib().or_hisq_deriv(_dims(dims), _coef(first), _coef(second), cn, eps, _p(g), _p(cfat), _p(clong), _p(d))
     return d
+
+
+
+# ---- gauge action, force and link update (hmc_oracle.c) -----------------
+
+def gauge_action(dims, u, plaq: float, rect: float = 0.0) -> float:
+    """gaugeAction1 (src/gauge/gaugeAction.nim:487-571) of (4, V, 3, 3) links."""
+    u = np.ascontiguousarray(u, dtype=np.complex128)
+    return lib().or_gauge_action(_dims(dims), plaq, rect, _p(u))
+
+
+def gauge_force(dims, u, plaq: float, rect: float = 0.0):
+    """gaugeForce (gaugeAction.nim:576-779): projectTAH(U f^dagger)."""
+    u = np.ascontiguousarray(u, dtype=np.complex128)
+    f = np.empty_like(u)
+    lib().or_gauge_force(_dims(dims), plaq, rect, _p(u), _p(f))
+    return f
+
+
+def exp_ah(m, eps: float = 1.0):
+    """expAH(eps m) (src/maths/matexp.nim:316-346) of (..., 3, 3)."""
+    m = np.ascontiguousarray(m, dtype=np.complex128)
+    out = np.empty_like(m)
+    lib().or_exp_ah(m.size // 9, _p(m), eps, _p(out))
+    return out
+
+
+def link_update(u, p, eps: float):
+    """axexpmuly(u, eps, p, u) (src/gauge/gaugeUtils.nim:452-459)."""
+    u = np.ascontiguousarray(u, dtype=np.complex128).copy()
+    p = np.ascontiguousarray(p, dtype=np.complex128)
+    lib().or_link_update(u.size // 9, _p(u), _p(p), eps)
+    return u

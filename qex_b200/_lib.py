@@ -66,6 +66,10 @@ class HisqCoefsC(C.Structure):
     ]
 
 
+class GaugeCoefsC(C.Structure):
+    _fields_ = [("plaq", C.c_double), ("rect", C.c_double)]
+
+
 class GaugeInfoC(C.Structure):
     _fields_ = [
         ("format", C.c_int),
@@ -135,6 +139,13 @@ SIGNATURES = {
     "qexstag_gauge_file_info": (I, [C.c_char_p, P]),
     "qexstag_gauge_read": (I, [P, C.c_char_p, P, I, P]),
     "qexstag_gauge_write": (I, [P, C.c_char_p, P, I, I, I, C.c_char_p, C.c_char_p]),
+    "qexstag_gauge_coefs_rect": (None, [P, D, D]),
+    "qexstag_gauge_action": (I, [P, P, P, I, DP]),
+    "qexstag_gauge_force": (I, [P, P, P, P, I]),
+    "qexstag_link_update": (I, [P, P, P, D, I]),
+    "qexstag_momenta_update": (I, [P, P, P, D, I]),
+    "qexstag_momenta_heatbath": (I, [P, P, C.c_ulonglong, C.c_ulonglong, I]),
+    "qexstag_kinetic_action": (I, [P, P, I, DP]),
 }
 
 _lib = None
