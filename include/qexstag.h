@@ -422,6 +422,42 @@ int qexstag_momenta_heatbath(qexstag_layout *l, double *p, unsigned long long se
 /* kineticAction (hmcAction.nim:248-255): 0.5 sum |p|^2 - 16 V. */
 int qexstag_kinetic_action(qexstag_layout *l, const double *p, int mem, double *t);
 
+/* ---- domain decomposition along t (QEX's rankGeom split with ShiftB
+   boundary exchanges: src/layout/shifts.nim:76-103, 263-294,
+   src/layout/qshifts.nim:23-177, src/comms/halo.nim) ----
+   The global lattice is split into nranks slabs of T = L3/nranks time
+   slices (T even, at least 6 for fat+Naik links and 4 for naive links);
+   rank r holds slices [r T, (r+1) T).  A rank's fields are its slab in the
+   V=1 order of the local lattice {L0, L1, L2, T} (qexstag_domain_local_dims):
+   links double[nlinks][Vloc][3][3][2] (host) or double2[nlinks][9][Vloc]
+   (device), phases folded in with global coordinates; colour vectors as
+   elsewhere.  Calls take the set of domains the calling process holds
+   (every rank in one process, or one rank per process); all processes make
+   the same calls in the same order. */
+typedef struct qexstag_domain_s qexstag_domain;
+int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nlinks, qexstag_domain **out);
+int qexstag_domain_destroy(qexstag_domain *d);
+int qexstag_domain_local_dims(const qexstag_domain *d, int dims[4]);
+/* All nranks domains in this process (rank order), on the current device:
+   boundaries are exchanged by device-to-device copies. */
+int qexstag_domain_connect_local(qexstag_domain *const *doms, int n);
+/* One domain per process: boundaries by NCCL send/receive and sums by NCCL
+   all-reduce over a communicator of nranks, from an id that rank 0 made
+   with qexstag_nccl_unique_id and every rank received. */
+int qexstag_nccl_unique_id(void *id128);
+int qexstag_domain_connect_nccl(qexstag_domain *d, const void *id128);
+/* Set each domain's links (links[k] for doms[k]) and exchange their
+   boundary slices. */
+int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const *links, int mem);
+/* stagD2ee on the decomposed lattice: r[k] even sites from x[k]. */
+int qexstag_domain_stagD2ee(qexstag_domain *const *doms, int n, double *const *r, const double *const *x, double m2,
+                            int mem);
+/* FP64 CG (cg.nim:55-272) for stagD2ee(m^2) y = b_e on the decomposed
+   lattice, zero start: x[k] receives y on even sites and zeros on odd
+   sites; st->r2 is the true relative residual over the whole lattice. */
+int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x, const double *const *b, double m,
+                           const qexstag_solver_params *p, qexstag_solver_stats *st, int mem);
+
 /* ---- benchmark hook (QEX's src/bench/benchStagProp.nim times the operator
    the same way, host timers around repeated calls) ---- */
 

@@ -146,6 +146,15 @@ SIGNATURES = {
     "qexstag_momenta_update": (I, [P, P, P, D, I]),
     "qexstag_momenta_heatbath": (I, [P, P, C.c_ulonglong, C.c_ulonglong, I]),
     "qexstag_kinetic_action": (I, [P, P, I, DP]),
+    "qexstag_domain_create": (I, [C.POINTER(C.c_int), I, I, I, C.POINTER(P)]),
+    "qexstag_domain_destroy": (I, [P]),
+    "qexstag_domain_local_dims": (I, [P, C.POINTER(C.c_int)]),
+    "qexstag_domain_connect_local": (I, [PP, I]),
+    "qexstag_nccl_unique_id": (I, [P]),
+    "qexstag_domain_connect_nccl": (I, [P, P]),
+    "qexstag_domain_links": (I, [PP, I, PP, I]),
+    "qexstag_domain_stagD2ee": (I, [PP, I, PP, PP, D, I]),
+    "qexstag_domain_solveEE": (I, [PP, I, PP, PP, D, P, P, I]),
 }
 
 _lib = None

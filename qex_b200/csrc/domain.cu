@@ -1,0 +1,580 @@
+// domain.cu -- domain decomposition of the staggered operator and its CG
+// along the time direction (scope row F3; QEX's rankGeom split with
+// ShiftB boundary exchanges, src/layout/shifts.nim:76-103, 263-294,
+// src/layout/qshifts.nim:23-177, src/comms/halo.nim).
+//
+// Rank r of R holds the time slices [r T, (r+1) T) of the global lattice
+// (T = L3 / R, even) as an extended lattice of T + 2h slices: h ghost slices
+// below and above, h = 6 for fat+Naik links and 2 for naive links (even, so
+// that a site's parity in the extended lattice is its global parity).  With
+// ghosts six slices deep the Schur operator's intermediate odd field is
+// correct on every slice the second half sweep reads, so one exchange of
+// the even input per application suffices and the library's FP64 Schur
+// kernels run unchanged on the extended lattice (the values they produce on
+// ghost slices are never used).  Reductions run over interior sites only,
+// are summed over the domains a process holds in rank order, and then over
+// processes.
+//
+// Neighbours held by the same process (several ranks on one device) are
+// exchanged by device-to-device copies; neighbours in other processes by
+// NCCL send/receive of the boundary slices into the receiver's ghost slices
+// and an NCCL all-reduce of the partial sums.  NCCL is resolved at run time
+// from the libnccl.so.2 already loaded in the process (the one torch
+// carries) or the system's, so the library does not link a second copy.
+#include <dlfcn.h>
+#include <nccl.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "lib.cuh"
+
+namespace qs {
+
+// ---- NCCL through dlsym ----
+struct NcclApi {
+  bool ok = false;
+  ncclResult_t (*getUniqueId)(ncclUniqueId *) = nullptr;
+  ncclResult_t (*commInitRank)(ncclComm_t *, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*commDestroy)(ncclComm_t) = nullptr;
+  ncclResult_t (*send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*allReduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                            cudaStream_t) = nullptr;
+  ncclResult_t (*groupStart)() = nullptr;
+  ncclResult_t (*groupEnd)() = nullptr;
+  const char *(*errorString)(ncclResult_t) = nullptr;
+};
+
+static NcclApi &nccl() {
+  static NcclApi api;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) return;
+    api.getUniqueId = (decltype(api.getUniqueId))dlsym(h, "ncclGetUniqueId");
+    api.commInitRank = (decltype(api.commInitRank))dlsym(h, "ncclCommInitRank");
+    api.commDestroy = (decltype(api.commDestroy))dlsym(h, "ncclCommDestroy");
+    api.send = (decltype(api.send))dlsym(h, "ncclSend");
+    api.recv = (decltype(api.recv))dlsym(h, "ncclRecv");
+    api.allReduce = (decltype(api.allReduce))dlsym(h, "ncclAllReduce");
+    api.groupStart = (decltype(api.groupStart))dlsym(h, "ncclGroupStart");
+    api.groupEnd = (decltype(api.groupEnd))dlsym(h, "ncclGroupEnd");
+    api.errorString = (decltype(api.errorString))dlsym(h, "ncclGetErrorString");
+    api.ok = api.getUniqueId && api.commInitRank && api.commDestroy && api.send && api.recv && api.allReduce &&
+             api.groupStart && api.groupEnd && api.errorString;
+  });
+  return api;
+}
+
+static int nccl_fail(ncclResult_t r, const char *what) {
+  return fail(QEXSTAG_ERR_CUDA, std::string(what) + ": " + (nccl().errorString ? nccl().errorString(r) : "NCCL"));
+}
+#define QS_NCCL(call)                                       \
+  do {                                                      \
+    ncclResult_t r_ = (call);                               \
+    if (r_ != ncclSuccess) return ::qs::nccl_fail(r_, #call); \
+  } while (0)
+
+}  // namespace qs
+
+struct qexstag_domain_s {
+  int gdims[4];
+  int nranks, rank, nl, h, T;
+  qexstag_layout_s *ext = nullptr;  // extended lattice (T + 2h slices)
+  qexstag_links_s *g = nullptr;     // links on the extended lattice
+  qexstag_domain_s *up = nullptr, *down = nullptr;  // in-process neighbours
+  ncclComm_t comm = nullptr;        // inter-process neighbours
+  bool connected = false;
+  std::vector<qs::Geom> local;      // geometry of the T-slice local lattice
+  double *dsum = nullptr;           // device scalar for all-reduce
+};
+
+namespace qs {
+
+// workspace slots of a domain's link handle
+enum DomainSlot {
+  kDmIn = kSlotLast + 700, kDmOut, kDmT, kDmFull, kDmX, kDmR, kDmP, kDmAp, kDmSoa, kDmLinks
+};
+
+static size_t slice_half(const qexstag_domain_s *d) {
+  return (size_t)d->gdims[0] * d->gdims[1] * d->gdims[2] / 2;
+}
+
+// one parity block's ghost exchange of ncomp component arrays, each with
+// stride V_ext, of the fields at base[k] of each domain of the set
+static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, int ncomp, int par) {
+  const size_t sh = slice_half(ds[0]);
+  for (int k = 0; k < n; k++) {
+    qexstag_domain_s *d = ds[k];
+    const size_t V = (size_t)d->ext->g.V, nh = (size_t)d->ext->g.nh;
+    const size_t cnt = d->h * sh;  // sites per face per component
+    if (d->comm) {
+      QS_NCCL(nccl().groupStart());
+      const int upr = (d->rank + 1) % d->nranks, dnr = (d->rank + d->nranks - 1) % d->nranks;
+      for (int c = 0; c < ncomp; c++) {
+        double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
+        // my top interior slices -> up's lower ghosts; my bottom -> down's upper
+        QS_NCCL(nccl().send(f + (size_t)d->T * sh, 2 * cnt, ncclDouble, upr, d->comm, stream()));
+        QS_NCCL(nccl().recv(f, 2 * cnt, ncclDouble, dnr, d->comm, stream()));
+        QS_NCCL(nccl().send(f + (size_t)d->h * sh, 2 * cnt, ncclDouble, dnr, d->comm, stream()));
+        QS_NCCL(nccl().recv(f + (size_t)(d->h + d->T) * sh, 2 * cnt, ncclDouble, upr, d->comm, stream()));
+      }
+      QS_NCCL(nccl().groupEnd());
+    } else {
+      // pull from the in-process neighbours
+      int ku = -1, kd = -1;
+      for (int j = 0; j < n; j++) {
+        if (ds[j] == d->up) ku = j;
+        if (ds[j] == d->down) kd = j;
+      }
+      if (ku < 0 || kd < 0) return fail(QEXSTAG_ERR_STATE, "domain: a neighbour is not in the call's domain set");
+      for (int c = 0; c < ncomp; c++) {
+        double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
+        const double2 *fd = base[kd] + (size_t)c * V + (size_t)par * nh;
+        const double2 *fu = base[ku] + (size_t)c * V + (size_t)par * nh;
+        QS_CUDA(cudaMemcpyAsync(f, fd + (size_t)d->down->T * sh, cnt * sizeof(double2), cudaMemcpyDeviceToDevice,
+                                stream()));
+        QS_CUDA(cudaMemcpyAsync(f + (size_t)(d->h + d->T) * sh, fu + (size_t)d->up->h * sh, cnt * sizeof(double2),
+                                cudaMemcpyDeviceToDevice, stream()));
+      }
+    }
+  }
+  return QEXSTAG_OK;
+}
+
+// sum of the n domains' device scalars (rank order), then over processes
+static int allreduce_sum(qexstag_domain_s *const *ds, int n, const double *vals, double *out) {
+  double s = 0;
+  for (int k = 0; k < n; k++) s += vals[k];
+  qexstag_domain_s *d = ds[0];
+  if (d->comm) {
+    QS_CUDA(cudaMemcpyAsync(d->dsum, &s, sizeof(double), cudaMemcpyHostToDevice, stream()));
+    QS_NCCL(nccl().allReduce(d->dsum, d->dsum, 1, ncclDouble, ncclSum, d->comm, stream()));
+    QS_CUDA(cudaMemcpyAsync(&s, d->dsum, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+    QS_CUDA(cudaStreamSynchronize(stream()));
+  }
+  *out = s;
+  return QEXSTAG_OK;
+}
+
+// local V=1 site order (T slices) <-> extended lattice (slices + h)
+__global__ void local_to_ext_kernel(Geom loc, Geom ext, int h, const double2 *in, size_t ins, double2 *out,
+                                    size_t outs, int ncomp, int to_ext) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < loc.V; i += gridDim.x * blockDim.x) {
+    const int par = i >= loc.nh ? 1 : 0;
+    int x[4], lex;
+    site_coords(loc, par, i - par * loc.nh, x, lex);
+    const int elex = x[0] + ext.L[0] * (x[1] + ext.L[1] * (x[2] + ext.L[2] * (x[3] + h)));
+    const int j = (elex >> 1) + par * ext.nh;  // same parity (h even)
+    for (int c = 0; c < ncomp; c++) {
+      if (to_ext)
+        out[(size_t)c * outs + j] = in[(size_t)c * ins + i];
+      else
+        out[(size_t)c * outs + i] = in[(size_t)c * ins + j];
+    }
+  }
+}
+
+__global__ void unit_links_kernel(size_t n, double2 *u) {
+  // n = nlinks * V sites of links; element e of link l at (l * 9 + e) * V + s
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < 9 * n; i += (size_t)gridDim.x * blockDim.x)
+    u[i] = make_double2(0.0, 0.0);
+}
+__global__ void unit_diag_kernel(int nl, int V, double2 *u) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < V; s += gridDim.x * blockDim.x)
+    for (int l = 0; l < nl; l++)
+      for (int e = 0; e < 9; e += 4) u[((size_t)l * 9 + e) * V + s] = make_double2(1.0, 0.0);
+}
+
+static int convert(qexstag_domain_s *d, const double2 *in, size_t ins, double2 *out, size_t outs, int ncomp,
+                   bool to_ext) {
+  const Geom &loc = d->local[0];
+  local_to_ext_kernel<<<grid_for(loc.V), kBlock, 0, stream()>>>(loc, d->ext->g, d->h, in, ins, out, outs, ncomp,
+                                                                to_ext ? 1 : 0);
+  note_launch();
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
+static int check_set(qexstag_domain_s *const *ds, int n) {
+  if (!ds || n < 1) return fail(QEXSTAG_ERR_ARG, "domain: empty domain set");
+  for (int k = 0; k < n; k++) {
+    if (!ds[k]) return fail(QEXSTAG_ERR_ARG, "domain: null domain");
+    if (!ds[k]->connected) return fail(QEXSTAG_ERR_STATE, "domain: not connected to its neighbours");
+    if (ds[k]->nl != ds[0]->nl || std::memcmp(ds[k]->gdims, ds[0]->gdims, sizeof ds[0]->gdims) ||
+        ds[k]->nranks != ds[0]->nranks)
+      return fail(QEXSTAG_ERR_ARG, "domain: domains of different lattices in one call");
+    if ((ds[k]->comm != nullptr) != (ds[0]->comm != nullptr))
+      return fail(QEXSTAG_ERR_ARG, "domain: in-process and NCCL domains in one call");
+  }
+  return runtime_ready();
+}
+
+// device copy (extended layout) of each domain's local full-lattice colour
+// vector; host fields [Vloc][3] or device [3][Vloc]
+struct ExtVec {
+  std::vector<double2 *> p;
+};
+
+static int vec_slot_get(qexstag_domain_s *d, int slot, double2 **out) {
+  void *q;
+  int rc = d->g->ws.get(slot, sizeof(double2) * 3 * (size_t)d->ext->g.V, &q);
+  if (rc) return rc;
+  *out = (double2 *)q;
+  return QEXSTAG_OK;
+}
+
+static int vec_in(qexstag_domain_s *d, int slot, const double *x, int mem, double2 **ext) {
+  int rc;
+  if ((rc = vec_slot_get(d, slot, ext))) return rc;
+  QS_CUDA(cudaMemsetAsync(*ext, 0, sizeof(double2) * 3 * (size_t)d->ext->g.V, stream()));
+  const size_t Vl = (size_t)d->local[0].V;
+  const double2 *src = (const double2 *)x;
+  if (mem == QEXSTAG_MEM_HOST) {
+    void *aos, *soa;
+    if ((rc = d->g->ws.get(kSlotAos, sizeof(double2) * 3 * Vl, &aos)) ||
+        (rc = d->g->ws.get(kDmSoa, sizeof(double2) * 3 * Vl, &soa)))
+      return rc;
+    QS_CUDA(cudaMemcpyAsync(aos, x, sizeof(double2) * 3 * Vl, cudaMemcpyHostToDevice, stream()));
+    if ((rc = aos_to_soa((const double *)aos, (double2 *)soa, (int)Vl, (int)Vl, 3))) return rc;
+    src = (const double2 *)soa;
+  }
+  return convert(d, src, Vl, *ext, d->ext->g.V, 3, true);
+}
+
+static int vec_out(qexstag_domain_s *d, const double2 *ext, double *x, int mem) {
+  const size_t Vl = (size_t)d->local[0].V;
+  int rc;
+  if (mem == QEXSTAG_MEM_DEVICE) return convert(d, ext, d->ext->g.V, (double2 *)x, Vl, 3, false);
+  void *aos, *soa;
+  if ((rc = d->g->ws.get(kSlotAos, sizeof(double2) * 3 * Vl, &aos)) ||
+      (rc = d->g->ws.get(kDmSoa, sizeof(double2) * 3 * Vl, &soa)))
+    return rc;
+  if ((rc = convert(d, ext, d->ext->g.V, (double2 *)soa, Vl, 3, false)) ||
+      (rc = soa_to_aos((const double2 *)soa, (double *)aos, (int)Vl, (int)Vl, 3)))
+    return rc;
+  QS_CUDA(cudaMemcpyAsync(x, aos, sizeof(double2) * 3 * Vl, cudaMemcpyDeviceToHost, stream()));
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+// interior even block of an extended field
+static VecD interior(qexstag_domain_s *d, double2 *f) {
+  return VecD{f + d->h * slice_half(d), d->ext->g.V};
+}
+static int interior_n(qexstag_domain_s *d) { return (int)(d->T * slice_half(d)); }
+
+// r = stagD2ee(m2) x on every domain: one exchange of x, then the Schur
+// kernels on the extended lattice
+static int schur_set(qexstag_domain_s *const *ds, int n, double2 *const *r, double2 *const *x, double2 *const *t,
+                     double m2) {
+  int rc;
+  if ((rc = exchange(ds, n, x, 3, 0))) return rc;
+  for (int k = 0; k < n; k++) {
+    const Geom &g = ds[k]->ext->g;
+    if ((rc = schur64(ds[k]->g, 0, VecD{r[k], g.V}, CVecD{x[k], g.V}, VecD{t[k] + g.nh, g.V}, m2))) return rc;
+  }
+  return QEXSTAG_OK;
+}
+
+static int dot_set(qexstag_domain_s *const *ds, int n, double2 *const *a, double2 *const *b, double *out) {
+  std::vector<double> v(n);
+  int rc;
+  for (int k = 0; k < n; k++) {
+    const VecD ia = interior(ds[k], a[k]), ib = interior(ds[k], b[k]);
+    if (a == b)
+      rc = vnorm2(cv(ia), interior_n(ds[k]), &v[k]);
+    else
+      rc = vredot(cv(ia), cv(ib), interior_n(ds[k]), &v[k]);
+    if (rc) return rc;
+  }
+  return allreduce_sum(ds, n, v.data(), out);
+}
+
+}  // namespace qs
+
+using namespace qs;
+
+extern "C" {
+
+int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nlinks, qexstag_domain **out) {
+  if (!global_dims || !out) return fail(QEXSTAG_ERR_ARG, "domain_create: null argument");
+  if (nlinks != 4 && nlinks != 8) return fail(QEXSTAG_ERR_ARG, "domain_create: nlinks must be 4 or 8");
+  if (nranks < 1 || rank < 0 || rank >= nranks) return fail(QEXSTAG_ERR_ARG, "domain_create: bad rank");
+  const int h = nlinks == 8 ? 6 : 2;
+  if (global_dims[3] % nranks) return fail(QEXSTAG_ERR_ARG, "domain_create: L3 is not a multiple of nranks");
+  const int T = global_dims[3] / nranks;
+  if (T % 2 || T < h || T < 4)
+    return fail(QEXSTAG_ERR_ARG, "domain_create: slab thickness must be even, at least 4 and at least the ghost "
+                                 "depth (6 fat+Naik, 2 naive)");
+  int rc = runtime_ready();
+  if (rc) return rc;
+  qexstag_domain_s *d = new (std::nothrow) qexstag_domain_s;
+  if (!d) return fail(QEXSTAG_ERR_ALLOC, "domain_create: out of host memory");
+  std::memcpy(d->gdims, global_dims, sizeof d->gdims);
+  d->nranks = nranks;
+  d->rank = rank;
+  d->nl = nlinks;
+  d->h = h;
+  d->T = T;
+  const int edims[4] = {global_dims[0], global_dims[1], global_dims[2], T + 2 * h};
+  const int ldims[4] = {global_dims[0], global_dims[1], global_dims[2], T};
+  qexstag_layout *le = nullptr, *ll = nullptr;
+  if ((rc = qexstag_layout_create(edims, &le)) || (rc = qexstag_layout_create(ldims, &ll))) {
+    if (le) qexstag_layout_destroy(le);
+    delete d;
+    return rc;
+  }
+  d->ext = le;
+  d->local.push_back(ll->g);
+  qexstag_layout_destroy(ll);
+  void *z = nullptr;
+  const size_t lb = sizeof(double2) * 9 * (size_t)le->g.V * nlinks;
+  if (cudaMalloc(&z, lb) != cudaSuccess || cudaMalloc((void **)&d->dsum, sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    if (z) cudaFree(z);
+    qexstag_layout_destroy(le);
+    delete d;
+    return fail(QEXSTAG_ERR_ALLOC, "domain_create: device allocation failed");
+  }
+  // unit links to start with (replaced by qexstag_domain_links)
+  unit_links_kernel<<<grid_for((long)le->g.V * nlinks), kBlock, 0, stream()>>>((size_t)le->g.V * nlinks,
+                                                                               (double2 *)z);
+  unit_diag_kernel<<<grid_for(le->g.V), kBlock, 0, stream()>>>(nlinks, le->g.V, (double2 *)z);
+  note_launch(2);
+  rc = qexstag_links_create(le, nlinks, (const double *)z, QEXSTAG_MEM_DEVICE, 1.0, &d->g);
+  cudaFree(z);
+  if (rc) {
+    cudaFree(d->dsum);
+    qexstag_layout_destroy(le);
+    delete d;
+    return rc;
+  }
+  *out = d;
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_destroy(qexstag_domain *d) {
+  if (!d) return QEXSTAG_OK;
+  if (d->comm && nccl().ok) nccl().commDestroy(d->comm);
+  if (d->g) qexstag_links_destroy(d->g);
+  if (d->ext) qexstag_layout_destroy(d->ext);
+  if (d->dsum) cudaFree(d->dsum);
+  delete d;
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_local_dims(const qexstag_domain *d, int dims[4]) {
+  if (!d || !dims) return fail(QEXSTAG_ERR_ARG, "domain_local_dims: null argument");
+  for (int k = 0; k < 3; k++) dims[k] = d->gdims[k];
+  dims[3] = d->T;
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_connect_local(qexstag_domain *const *doms, int n) {
+  if (!doms || n < 1) return fail(QEXSTAG_ERR_ARG, "domain_connect_local: empty set");
+  for (int k = 0; k < n; k++) {
+    if (!doms[k] || doms[k]->nranks != n || doms[k]->rank != k)
+      return fail(QEXSTAG_ERR_ARG, "domain_connect_local: pass every rank's domain, in rank order");
+    if (doms[k]->nl != doms[0]->nl || std::memcmp(doms[k]->gdims, doms[0]->gdims, sizeof doms[0]->gdims))
+      return fail(QEXSTAG_ERR_ARG, "domain_connect_local: domains of different lattices");
+  }
+  for (int k = 0; k < n; k++) {
+    doms[k]->up = doms[(k + 1) % n];
+    doms[k]->down = doms[(k + n - 1) % n];
+    doms[k]->connected = true;
+  }
+  return QEXSTAG_OK;
+}
+
+int qexstag_nccl_unique_id(void *id) {
+  if (!id) return fail(QEXSTAG_ERR_ARG, "nccl_unique_id: null argument");
+  if (!nccl().ok) return fail(QEXSTAG_ERR_STATE, "nccl_unique_id: libnccl.so.2 not available");
+  QS_NCCL(nccl().getUniqueId((ncclUniqueId *)id));
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_connect_nccl(qexstag_domain *d, const void *id) {
+  if (!d || !id) return fail(QEXSTAG_ERR_ARG, "domain_connect_nccl: null argument");
+  if (!nccl().ok) return fail(QEXSTAG_ERR_STATE, "domain_connect_nccl: libnccl.so.2 not available");
+  ncclUniqueId u;
+  std::memcpy(&u, id, sizeof u);
+  QS_NCCL(nccl().commInitRank(&d->comm, d->nranks, u, d->rank));
+  d->connected = true;
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const *links, int mem) {
+  int rc;
+  if ((rc = check_set(doms, n))) return rc;
+  if (!links || (mem != QEXSTAG_MEM_HOST && mem != QEXSTAG_MEM_DEVICE))
+    return fail(QEXSTAG_ERR_ARG, "domain_links: bad arguments");
+  std::vector<double2 *> base(n);
+  for (int k = 0; k < n; k++) {
+    qexstag_domain_s *d = doms[k];
+    if (!links[k]) return fail(QEXSTAG_ERR_ARG, "domain_links: null links");
+    const size_t Vl = (size_t)d->local[0].V, Ve = (size_t)d->ext->g.V;
+    const double2 *src = (const double2 *)links[k];
+    void *soa = nullptr;
+    if (mem == QEXSTAG_MEM_HOST) {
+      void *aos;
+      if ((rc = d->g->ws.get(kSlotAos, sizeof(double2) * 9 * Vl, &aos)) ||
+          (rc = d->g->ws.get(kDmLinks, sizeof(double2) * 9 * Vl * d->nl, &soa)))
+        return rc;
+      for (int l = 0; l < d->nl; l++) {
+        QS_CUDA(cudaMemcpyAsync(aos, links[k] + (size_t)l * 18 * Vl, sizeof(double2) * 9 * Vl,
+                                cudaMemcpyHostToDevice, stream()));
+        if ((rc = aos_to_soa((const double *)aos, (double2 *)soa + (size_t)l * 9 * Vl, (int)Vl, (int)Vl, 9)))
+          return rc;
+      }
+      src = (const double2 *)soa;
+    }
+    for (int l = 0; l < d->nl; l++)
+      if ((rc = convert(d, src + (size_t)l * 9 * Vl, Vl, d->g->u64 + (size_t)l * 9 * Ve, Ve, 9, true))) return rc;
+    base[k] = d->g->u64;
+  }
+  // ghosts of every link component, both parities
+  const int ncomp = 9 * doms[0]->nl;
+  for (int par = 0; par < 2; par++)
+    if ((rc = exchange(doms, n, base.data(), ncomp, par))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_stagD2ee(qexstag_domain *const *doms, int n, double *const *r, const double *const *x, double m2,
+                            int mem) {
+  int rc;
+  if ((rc = check_set(doms, n))) return rc;
+  if (!r || !x) return fail(QEXSTAG_ERR_ARG, "domain_stagD2ee: null fields");
+  std::vector<double2 *> xe(n), re(n), te(n);
+  for (int k = 0; k < n; k++) {
+    if ((rc = vec_in(doms[k], kDmIn, x[k], mem, &xe[k])) || (rc = vec_slot_get(doms[k], kDmOut, &re[k])) ||
+        (rc = vec_slot_get(doms[k], kDmT, &te[k])))
+      return rc;
+  }
+  if ((rc = schur_set(doms, n, re.data(), xe.data(), te.data(), m2))) return rc;
+  for (int k = 0; k < n; k++) {
+    // only the even sites of r are written, as stagD2ee does
+    const Geom &loc = doms[k]->local[0];
+    const size_t Ve = (size_t)doms[k]->ext->g.V;
+    if (mem == QEXSTAG_MEM_DEVICE) {
+      double2 *full;
+      if ((rc = vec_slot_get(doms[k], kDmFull, &full)) || (rc = convert(doms[k], re[k], Ve, full, loc.V, 3, false)))
+        return rc;
+      for (int c = 0; c < 3; c++)
+        QS_CUDA(cudaMemcpyAsync((double2 *)r[k] + (size_t)c * loc.V, full + (size_t)c * loc.V,
+                                sizeof(double2) * loc.nh, cudaMemcpyDeviceToDevice, stream()));
+    } else {
+      double *rh = r[k];
+      std::vector<double> keep((size_t)6 * (loc.V - loc.nh));
+      std::memcpy(keep.data(), rh + (size_t)6 * loc.nh, keep.size() * sizeof(double));
+      if ((rc = vec_out(doms[k], re[k], rh, mem))) return rc;
+      std::memcpy(rh + (size_t)6 * loc.nh, keep.data(), keep.size() * sizeof(double));
+    }
+  }
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+// CG for stagD2ee(m^2) y = b_e across the domains (cg.nim:55-272, cpNone),
+// FP64 from a zero start; x receives y on even sites and zeros on odd sites.
+int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x, const double *const *b, double m,
+                           const qexstag_solver_params *p, qexstag_solver_stats *st_out, int mem) {
+  int rc;
+  if ((rc = check_set(doms, n))) return rc;
+  if (!x || !b || !p) return fail(QEXSTAG_ERR_ARG, "domain_solveEE: null argument");
+  const double m2 = m * m;
+  std::vector<double2 *> bv(n), xv(n), rv(n), pv(n), ap(n), tv(n);
+  for (int k = 0; k < n; k++) {
+    qexstag_domain_s *d = doms[k];
+    if ((rc = vec_in(d, kDmIn, b[k], mem, &bv[k])) || (rc = vec_slot_get(d, kDmX, &xv[k])) ||
+        (rc = vec_slot_get(d, kDmR, &rv[k])) || (rc = vec_slot_get(d, kDmP, &pv[k])) ||
+        (rc = vec_slot_get(d, kDmAp, &ap[k])) || (rc = vec_slot_get(d, kDmT, &tv[k])))
+      return rc;
+    const size_t bytes = sizeof(double2) * 3 * (size_t)d->ext->g.V;
+    QS_CUDA(cudaMemsetAsync(xv[k], 0, bytes, stream()));
+    QS_CUDA(cudaMemsetAsync(pv[k], 0, bytes, stream()));
+    QS_CUDA(cudaMemsetAsync(rv[k], 0, bytes, stream()));
+    const int ni = interior_n(d);
+    if ((rc = vcopy(interior(d, rv[k]), cv(interior(d, bv[k])), ni)) ||
+        (rc = vcopy(interior(d, pv[k]), cv(interior(d, bv[k])), ni)))
+      return rc;
+  }
+  double b2 = 0, r2 = 0, pAp = 0;
+  if ((rc = dot_set(doms, n, bv.data(), bv.data(), &b2))) return rc;
+  if (!std::isfinite(b2)) return fail(QEXSTAG_ERR_NAN, "domain_solveEE: source is not finite");
+  r2 = b2;
+  const double r2stop = p->r2req * b2;
+  const int maxits = p->maxits > 0 ? p->maxits : 50000;
+  int its = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, stream());
+  while (r2 > r2stop && its < maxits) {
+    if ((rc = schur_set(doms, n, ap.data(), pv.data(), tv.data(), m2))) break;
+    if ((rc = dot_set(doms, n, pv.data(), ap.data(), &pAp))) break;
+    const double alpha = r2 / pAp;
+    for (int k = 0; k < n && !rc; k++) {
+      qexstag_domain_s *d = doms[k];
+      const int ni = interior_n(d);
+      rc = vaxpy(interior(d, xv[k]), alpha, cv(interior(d, pv[k])), ni);
+      if (!rc) rc = vaxpy(interior(d, rv[k]), -alpha, cv(interior(d, ap[k])), ni);
+    }
+    if (rc) break;
+    double r2n;
+    if ((rc = dot_set(doms, n, rv.data(), rv.data(), &r2n))) break;
+    if (!std::isfinite(r2n)) {
+      rc = fail(QEXSTAG_ERR_NAN, "domain_solveEE: NaN residual");
+      break;
+    }
+    const double beta = r2n / r2;
+    r2 = r2n;
+    its++;
+    for (int k = 0; k < n && !rc; k++)
+      rc = vxpay(interior(doms[k], pv[k]), cv(interior(doms[k], rv[k])), beta, interior_n(doms[k]));
+    if (rc) break;
+  }
+  cudaEventRecord(e1, stream());
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  // true residual
+  for (int k = 0; k < n; k++) {
+    // odd sites of the solution are zero
+    const size_t Ve = (size_t)doms[k]->ext->g.V, nh = (size_t)doms[k]->ext->g.nh;
+    for (int c = 0; c < 3; c++) QS_CUDA(cudaMemsetAsync(xv[k] + c * Ve + nh, 0, sizeof(double2) * nh, stream()));
+  }
+  if ((rc = schur_set(doms, n, ap.data(), xv.data(), tv.data(), m2))) return rc;
+  for (int k = 0; k < n; k++) {
+    const int ni = interior_n(doms[k]);
+    if ((rc = vsub(interior(doms[k], rv[k]), cv(interior(doms[k], bv[k])), cv(interior(doms[k], ap[k])), ni)))
+      return rc;
+  }
+  double rt2 = 0;
+  if ((rc = dot_set(doms, n, rv.data(), rv.data(), &rt2))) return rc;
+  for (int k = 0; k < n; k++)
+    if ((rc = vec_out(doms[k], xv[k], x[k], mem))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  if (st_out) {
+    std::memset(st_out, 0, sizeof(*st_out));
+    st_out->calls = 1;
+    st_out->iterations = its;
+    st_out->outer_iterations = 1;
+    st_out->seconds = ms * 1e-3;
+    st_out->flops = (double)(doms[0]->nl * 4 * 72 + 60) * ((double)doms[0]->gdims[0] * doms[0]->gdims[1] *
+                                                           doms[0]->gdims[2] * doms[0]->gdims[3] / 2) * its;
+    st_out->r2 = b2 > 0 ? rt2 / b2 : 0.0;
+  }
+  return rt2 <= r2stop * 1.0000001 ? QEXSTAG_OK : QEXSTAG_NOT_CONVERGED;
+}
+
+}  // extern "C"

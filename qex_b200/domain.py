@@ -1,0 +1,110 @@
+"""Domain decomposition along t through the C ABI (qexstag_domain_*): QEX's
+rank split of the lattice (rankGeom; src/layout/shifts.nim, qshifts.nim)
+with ghost-slice exchanges.  A process holds either every rank's domain
+(one device, exchanges by device copies) or one (one rank per GPU,
+exchanges and sums by NCCL).
+
+Global host fields are split into rank slabs here for convenience: links
+(nlinks, V, 3, 3) and colour vectors (V, 3) in the global V=1 order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from . import fields as F
+from . import stag as S
+
+
+def _arr(ptrs):
+    return (C.c_void_p * len(ptrs))(*ptrs)
+
+
+class DomainSet:
+    """The domains this process holds: ranks[0..] of an nranks split."""
+
+    def __init__(self, global_dims, nranks: int, nlinks: int, ranks=None, nccl_id: bytes | None = None):
+        S.init(0)
+        self.lib = L.load()
+        self.gdims = tuple(int(d) for d in global_dims)
+        self.nranks = nranks
+        self.nl = nlinks
+        self.ranks = list(range(nranks)) if ranks is None else list(ranks)
+        self.handles = []
+        dims = (C.c_int * 4)(*self.gdims)
+        for r in self.ranks:
+            h = C.c_void_p()
+            L.check(self.lib.qexstag_domain_create(dims, nranks, r, nlinks, C.byref(h)), "domain_create")
+            self.handles.append(h)
+        ld = (C.c_int * 4)()
+        L.check(self.lib.qexstag_domain_local_dims(self.handles[0], ld), "domain_local_dims")
+        self.ldims = tuple(ld)
+        if nccl_id is None:
+            L.check(self.lib.qexstag_domain_connect_local(self._set(), len(self.handles)), "domain_connect_local")
+        else:
+            buf = C.create_string_buffer(bytes(nccl_id), 128)
+            for h in self.handles:
+                L.check(self.lib.qexstag_domain_connect_nccl(h, buf), "domain_connect_nccl")
+        # global index of each local site, per rank
+        c = F.coords(self.ldims)
+        self.gidx = []
+        for r in self.ranks:
+            g = c.copy()
+            g[:, 3] += r * self.ldims[3]
+            self.gidx.append(F.index_of(self.gdims, g))
+
+    def _set(self):
+        return _arr([h.value for h in self.handles])
+
+    def __del__(self):
+        try:
+            for h in getattr(self, "handles", []):
+                self.lib.qexstag_domain_destroy(h)
+            self.handles = []
+        except Exception:
+            pass
+
+    def split_links(self, g: np.ndarray):
+        return [np.ascontiguousarray(g[:, ix]) for ix in self.gidx]
+
+    def split_vector(self, x: np.ndarray):
+        return [np.ascontiguousarray(x[ix]) for ix in self.gidx]
+
+    def gather_vector(self, parts, out: np.ndarray):
+        for ix, p in zip(self.gidx, parts):
+            out[ix] = p
+        return out
+
+    def set_links(self, g: np.ndarray) -> None:
+        self._links = self.split_links(np.ascontiguousarray(g, dtype=np.complex128))
+        L.check(self.lib.qexstag_domain_links(self._set(), len(self.handles),
+                                              _arr([a.ctypes.data for a in self._links]), L.MEM_HOST),
+                "domain_links")
+
+    def stagD2ee(self, r: np.ndarray, x: np.ndarray, m2: float) -> None:
+        xs = self.split_vector(x)
+        rs = self.split_vector(r)
+        L.check(self.lib.qexstag_domain_stagD2ee(self._set(), len(self.handles), _arr([a.ctypes.data for a in rs]),
+                                                 _arr([a.ctypes.data for a in xs]), m2, L.MEM_HOST),
+                "domain_stagD2ee")
+        self.gather_vector(rs, r)
+
+    def solveEE(self, x: np.ndarray, b: np.ndarray, m: float, sp: S.SolverParams) -> None:
+        bs = self.split_vector(b)
+        xs = [np.zeros_like(v) for v in bs]
+        st = L.SolverStatsC()
+        pc = sp.c_params()
+        rc = self.lib.qexstag_domain_solveEE(self._set(), len(self.handles), _arr([a.ctypes.data for a in xs]),
+                                             _arr([a.ctypes.data for a in bs]), m, C.byref(pc), C.byref(st),
+                                             L.MEM_HOST)
+        L.check(rc, "domain_solveEE")
+        sp.take(st, rc)
+        self.gather_vector(xs, x)
+
+
+def nccl_unique_id() -> bytes:
+    buf = C.create_string_buffer(128)
+    L.check(L.load().qexstag_nccl_unique_id(buf), "nccl_unique_id")
+    return buf.raw
