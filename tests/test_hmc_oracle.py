@@ -32,7 +32,9 @@ def test_force_is_the_derivative_of_the_action(dims, rect):
     u = F.gauge_warm(dims, 0.5, 4)
     plaq = 5.6 * (1 - 8 * rect / 5.6) if rect else 5.6
     f = O.gauge_force(dims, u, plaq, rect)
-    eps = 1e-5
+    # the action is ~1e4: its rounding (~1e-11) over 2 eps bounds the
+    # difference from below, the eps^2 truncation from above
+    eps = 1e-4
     for _ in range(8):
         mu, x = int(rng.integers(0, 4)), int(rng.integers(0, V))
         T = F.rand_tah(1, rng)[0]
@@ -43,7 +45,7 @@ def test_force_is_the_derivative_of_the_action(dims, rect):
             vals.append(O.gauge_action(dims, up, plaq, rect))
         fd = (vals[0] - vals[1]) / (2 * eps)
         an = np.trace(np.conj(T).T @ f[mu, x]).real
-        assert abs(fd - an) < 1e-7 * max(1.0, abs(an)), (mu, x, fd, an)
+        assert abs(fd - an) < 2e-6 * max(1.0, abs(an)), (mu, x, fd, an)
     # traceless anti-Hermitian
     assert np.abs(f + np.conj(np.swapaxes(f, -1, -2))).max() < 1e-13
     assert np.abs(np.trace(f, axis1=-2, axis2=-1)).max() < 1e-13
