@@ -119,6 +119,13 @@ __device__ __forceinline__ float2 cjmadd(float2 acc, float2 a, float2 b) {
   return acc;
 }
 
+// Programmatic dependent launch: block until the kernel before this one in
+// the stream has completed and its writes are visible.  Kernels that start
+// with it may be launched with launch_pdl, which lets the GPU schedule them
+// while the previous kernel drains; under an ordinary launch it returns at
+// once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // read-only, streaming loads
 __device__ __forceinline__ double2 ldg(const double2 *p) { return __ldg(p); }
 __device__ __forceinline__ float2 ldg(const float2 *p) { return __ldg(p); }
@@ -255,6 +262,23 @@ double *host_results();  // pinned host mirror
 // count of kernels this thread has launched through the library
 void note_launch(int n = 1);
 long long launch_count();
+
+// launch a kernel that begins with pdl_wait() with programmatic stream
+// serialisation on the library's stream
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, int block, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream();
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, ((KArgs)args)...);
+}
 
 inline int grid_for(long n, int block = kBlock, int per_sm = 8) {
   long b = (n + block - 1) / block;

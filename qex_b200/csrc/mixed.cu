@@ -313,6 +313,7 @@ struct DslashArgsLo {
 
 template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
 __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel(const DslashArgsLo A) {
+  pdl_wait();
   if (A.halt != nullptr && mx_halt(A.halt)) return;
   const Geom &g = A.g;
   const int nh = g.nh;
@@ -442,13 +443,12 @@ static int lo_grid(int nh) {
 
 template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP>
 static void launch_lo(const DslashArgsLo &A, int) {
-  if (NL == 8 && A.L.recon12) {
-    dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>
-        <<<lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, 0, stream()>>>(A);
-  } else {
-    dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>
-        <<<lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, 0, stream()>>>(A);
-  }
+  if (NL == 8 && A.L.recon12)
+    launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>,
+               lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, A);
+  else
+    launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>,
+               lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, A);
   note_launch();
 }
 
@@ -560,6 +560,7 @@ template <int PREC>
 __global__ void __launch_bounds__(kBlock)
     mx_update_kernel(float2 *__restrict__ rs, float2 *__restrict__ xs, const float2 *__restrict__ ap,
                      const void *p, int n, MxState *st, double *partials, unsigned *ticket) {
+  pdl_wait();
   if (mx_halt(st)) return;
   const float alpha = (float)st->alpha;
   double s = 0.0;
@@ -607,6 +608,7 @@ __global__ void __launch_bounds__(kBlock)
 
 template <int PREC>
 __global__ void mx_p_kernel(const float2 *__restrict__ rs, void *p, int n, const MxState *st) {
+  pdl_wait();
   if (mx_halt(st)) return;
   const float beta = (float)st->beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -765,9 +767,9 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   for (;;) {
     for (int i = 0; i < every; i++) {
       if ((rc = schur_lo(g, PREC, par, ap, pp, pt, m2, 1, st, st, nullptr))) return rc;
-      mx_update_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, xs, ap, pp, nh, st, red_partials(),
-                                                            red_tickets());
-      mx_p_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
+      launch_pdl(mx_update_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)pp, nh, st,
+                 red_partials(), red_tickets());
+      launch_pdl(mx_p_kernel<VP>, egrid, kBlock, (const float2 *)rs, (void *)pp, nh, (const MxState *)st);
       note_launch(2);
     }
     QS_LAUNCH_CHECK();
