@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(kBlock)
 
 __global__ void cg_p_kernel(const double2 *__restrict__ r, int rs, double2 *__restrict__ p, int ps,
                             int n, const CgState *st) {
+  pdl_wait();
   if (st->done) return;
   const bool first = (st->itn == 0);
   const double beta = st->beta;
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(kBlock)
     cg_xr_kernel(double2 *__restrict__ x, int xs, double2 *__restrict__ r, int rs,
                  const double2 *__restrict__ p, int ps, const double2 *__restrict__ ap, int aps,
                  int n, CgState *st, double *partials, unsigned *ticket) {
+  pdl_wait();
   if (st->done) return;
   const double alpha = st->alpha;
   double s = 0.0;
@@ -156,12 +158,12 @@ int cg64(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, 
   const int pgrid = grid_for(nh, kBlock, 8);
   for (;;) {
     for (int i = 0; i < every; i++) {
-      cg_p_kernel<<<pgrid, kBlock, 0, stream()>>>(r.p, r.stride, p.p, p.stride, nh, st);
+      launch_pdl(cg_p_kernel, pgrid, kBlock, (const double2 *)r.p, r.stride, p.p, p.stride, nh,
+                 (const CgState *)st);
       note_launch();
       if ((rc = schur64(g, par, ap, cv(p), t, m2, kRedCgPAp, st, &st->done))) return rc;
-      cg_xr_kernel<<<grid, kBlock, 0, stream()>>>(x.p, x.stride, r.p, r.stride, p.p, p.stride,
-                                                  ap.p, ap.stride, nh, st, red_partials(),
-                                                  red_tickets());
+      launch_pdl(cg_xr_kernel, grid, kBlock, x.p, x.stride, r.p, r.stride, (const double2 *)p.p, p.stride,
+                 (const double2 *)ap.p, ap.stride, nh, st, red_partials(), red_tickets());
       note_launch();
     }
     QS_LAUNCH_CHECK();

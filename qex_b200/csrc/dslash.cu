@@ -42,6 +42,7 @@ struct DslashArgs64 {
 
 template <int NL, int HOP, int INIT, int RED>
 __global__ void __launch_bounds__(kBlock) dslash64_kernel(const DslashArgs64 A) {
+  pdl_wait();
   if (A.done != nullptr && *A.done) return;
   const Geom &g = A.g;
   const int nh = g.nh;
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(kBlock) dslash64_kernel(const DslashArgs64 A) 
 
 template <int NL, int HOP, int INIT, int RED>
 static void launch64(const DslashArgs64 &A, int grid) {
-  dslash64_kernel<NL, HOP, INIT, RED><<<grid, kBlock, 0, stream()>>>(A);
+  launch_pdl(dslash64_kernel<NL, HOP, INIT, RED>, grid, kBlock, A);
   note_launch();
 }
 
