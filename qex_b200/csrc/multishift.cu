@@ -6,8 +6,9 @@
 //   cgm_ee: (A + sigma_k) y_jk = b_j for up to 8 right-hand sides, with an
 //     FP32 multi-right-hand-side Dslash that reads each link once per site for
 //     all of them, shifts dropped once their residual |zeta_k| |r| meets the
-//     target, then FP64 true residuals and mixed-precision refinement of every
-//     (j, k) still above it.
+//     target, then FP64 true residuals and, for every shift, a
+//     multi-right-hand-side FP32 CG on the residuals of the right-hand sides
+//     still above it (FP64 defect correction).
 // All scalars (alpha, beta, zeta recurrences) live on the device in FP64.
 #include <algorithm>
 #include <cmath>
@@ -46,9 +47,17 @@ struct CgmVecs {
 };
 
 // ---------------------------------------------------------------------------
-// FP32 multi-right-hand-side Dslash: each thread one site, all right-hand
-// sides; each link read once per site and applied to every vector.
+// FP32 multi-right-hand-side Dslash: a block is kMrhsGroups warp-uniform
+// groups of kMrhsSites sites; group q applies the operator to right-hand
+// sides q*kMrhsPer .. q*kMrhsPer+kMrhsPer-1 of its sites.  Every group loads
+// the same links, so each link comes from HBM once per site and from L1 for
+// the other groups, while each right-hand side's vector loads stay
+// coalesced across the warp.
 // ---------------------------------------------------------------------------
+
+constexpr int kMrhsPer = 4;                       // right-hand sides per thread
+constexpr int kMrhsGroups = kMaxRhs / kMrhsPer;   // 2
+constexpr int kMrhsSites = kBlock / kMrhsGroups;  // 128 sites per block step
 
 struct MrhsArgs {
   Geom g;
@@ -67,24 +76,28 @@ struct MrhsArgs {
 };
 
 template <int NL, int HOP, int INIT, int RED, int R12>
-__global__ void __launch_bounds__(kBlock) dslash_mrhs_kernel(const MrhsArgs A) {
+__global__ void __launch_bounds__(kBlock, 2) dslash_mrhs_kernel(const MrhsArgs A) {
+  pdl_wait();
   if (A.st->done) return;
   const Geom &g = A.g;
   const int nh = g.nh;
   const size_t V = (size_t)g.V;
   const size_t in_base = (size_t)(1 - A.po) * nh;
   const size_t out_base = (size_t)A.po * nh;
-  double dot[kMaxRhs];
+  const int grp = threadIdx.x / kMrhsSites;
+  const int j0 = grp * kMrhsPer;
+  double dot[kMrhsPer];
 #pragma unroll
-  for (int j = 0; j < kMaxRhs; j++) dot[j] = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+  for (int q = 0; q < kMrhsPer; q++) dot[q] = 0.0;
+  for (int k = blockIdx.x * kMrhsSites + (threadIdx.x % kMrhsSites); k < nh; k += gridDim.x * kMrhsSites) {
+    if (j0 >= A.nr) break;
     int x[4], lex;
     site_coords(g, A.po, k, x, lex);
-    float2 acc[kMaxRhs][3];
+    float2 acc[kMrhsPer][3];
 #pragma unroll
-    for (int j = 0; j < kMaxRhs; j++)
+    for (int q = 0; q < kMrhsPer; q++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) acc[j][c] = make_float2(0.f, 0.f);
+      for (int c = 0; c < 3; c++) acc[q][c] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int l = 0; l < NL; l++) {
       const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
@@ -104,7 +117,8 @@ __global__ void __launch_bounds__(kBlock) dslash_mrhs_kernel(const MrhsArgs A) {
         load_link18<kF32>(A.L.f32_fat, A.L.f32_fat_tail, nullptr, nullptr, f, in_base + jb, V, ub);
       }
 #pragma unroll
-      for (int j = 0; j < kMaxRhs; j++) {
+      for (int q = 0; q < kMrhsPer; q++) {
+        const int j = j0 + q;
         if (j < A.nr) {
           const float2 *xj = A.xin + (size_t)j * A.irs;
           float2 v[3], w[3];
@@ -115,31 +129,32 @@ __global__ void __launch_bounds__(kBlock) dslash_mrhs_kernel(const MrhsArgs A) {
           }
 #pragma unroll
           for (int i = 0; i < 3; i++) {
-            float2 t = make_float2(0.f, 0.f), q = make_float2(0.f, 0.f);
+            float2 t = make_float2(0.f, 0.f), u = make_float2(0.f, 0.f);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
               t = cmadd(t, uf[3 * i + c], v[c]);
-              q = cjmadd(q, ub[3 * c + i], w[c]);
+              u = cjmadd(u, ub[3 * c + i], w[c]);
             }
             if (HOP > 0) {
-              acc[j][i].x += t.x - q.x;
-              acc[j][i].y += t.y - q.y;
+              acc[q][i].x += t.x - u.x;
+              acc[q][i].y += t.y - u.y;
             } else {
-              acc[j][i].x -= t.x - q.x;
-              acc[j][i].y -= t.y - q.y;
+              acc[q][i].x -= t.x - u.x;
+              acc[q][i].y -= t.y - u.y;
             }
           }
         }
       }
     }
 #pragma unroll
-    for (int j = 0; j < kMaxRhs; j++) {
+    for (int q = 0; q < kMrhsPer; q++) {
+      const int j = j0 + q;
       if (j < A.nr) {
         float2 *oj = A.out + (size_t)j * A.ors;
         float d = 0.f;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          float2 o = acc[j][c];
+          float2 o = acc[q][c];
           if (INIT) {
             float2 s = __ldcg(A.xs + (size_t)j * A.srs + (size_t)c * nh + k);
             o.x = fmaf(A.b, s.x, o.x);
@@ -148,13 +163,17 @@ __global__ void __launch_bounds__(kBlock) dslash_mrhs_kernel(const MrhsArgs A) {
           }
           oj[(size_t)c * nh + k] = o;
         }
-        if (RED) dot[j] += (double)d;
+        if (RED) dot[q] += (double)d;
       }
     }
   }
   if (RED) {
+    // each right-hand side's sum from its group's threads (static indices)
+    double all[kMaxRhs];
+#pragma unroll
+    for (int j = 0; j < kMaxRhs; j++) all[j] = (j / kMrhsPer == grp) ? dot[j % kMrhsPer] : 0.0;
     double s[kMaxRhs];
-    if (grid_reduce<kMaxRhs>(dot, A.partials, A.ticket, s) && threadIdx.x == 0)
+    if (grid_reduce<kMaxRhs>(all, A.partials, A.ticket, s) && threadIdx.x == 0)
       for (int j = 0; j < A.nr; j++) A.wst->pAp[j] = s[j];
   }
 }
@@ -171,7 +190,7 @@ static void mrhs_pair(MrhsArgs A, int par, const float2 *p, size_t prs, float2 *
   A.out = t;
   A.ors = vs;
   A.b = 0.f;
-  dslash_mrhs_kernel<NL, 1, 0, 0, R12><<<grid, kBlock, 0, stream()>>>(A);
+  launch_pdl(dslash_mrhs_kernel<NL, 1, 0, 0, R12>, grid, kBlock, A);
   A.po = par;
   A.xin = t;
   A.irs = vs;
@@ -180,7 +199,7 @@ static void mrhs_pair(MrhsArgs A, int par, const float2 *p, size_t prs, float2 *
   A.out = ap;
   A.ors = vs;
   A.b = b4m2;
-  dslash_mrhs_kernel<NL, -1, 1, 1, R12><<<grid, kBlock, 0, stream()>>>(A);
+  launch_pdl(dslash_mrhs_kernel<NL, -1, 1, 1, R12>, grid, kBlock, A);
   note_launch(2);
 }
 
@@ -197,8 +216,10 @@ static int schur_mrhs(const qexstag_links_s *g, int par, int nr, const float2 *p
   A.wst = st;
   A.partials = red_partials();
   A.ticket = red_tickets();
-  int grid = grid_for(geo.nh, kBlock, 4);
+  // blocks step over kMrhsSites sites; at most kMaxRedBlocks*8/kMaxRhs for the reduction
+  int grid = (int)std::min<long>(((long)geo.nh + kMrhsSites - 1) / kMrhsSites, (long)num_sms() * 4);
   if (grid * kMaxRhs > kMaxRedBlocks * 8) grid = kMaxRedBlocks * 8 / kMaxRhs;
+  if (grid < 1) grid = 1;
   const float b4 = (float)(4.0 * m2);
   if (g->nl == 8) {
     if (g->low.recon12)
@@ -620,8 +641,6 @@ int solve_multishift(qexstag_links_s *g, int nmass, double2 *const *xs, const do
   return (r2 > r2stop) ? QEXSTAG_NOT_CONVERGED : QEXSTAG_OK;
 }
 
-int cg_mixed(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, int maxits, int sloppy,
-             double delta, CgOut *out, int *reliable);
 int cg64(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, int maxits, CgOut *out);
 
 // (A + sigma) y on even sites, FP64: r = b - (A + sigma) y, returns |r|^2
@@ -684,46 +703,106 @@ int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nr
   }
   st->outer_iterations += 1;
   // FP64 true residuals; refine every (j, k) above the target
-  void *pr, *pt, *pd;
-  if ((rc = g->ws.get(kSlotMs0 + 50, sizeof(double2) * 3 * (size_t)nh, &pr)) ||
-      (rc = g->ws.get(kSlotMs0 + 51, sizeof(double2) * 3 * (size_t)nh, &pt)) ||
-      (rc = g->ws.get(kSlotMs0 + 52, sizeof(double2) * 3 * (size_t)nh, &pd)))
-    return rc;
-  double2 *r = (double2 *)pr, *t = (double2 *)pt, *d = (double2 *)pd;
+  const size_t vb = sizeof(double2) * 3 * (size_t)nh;
+  std::vector<double> b2(nrhs);
+  for (int j = 0; j < nrhs; j++) {
+    if ((rc = vnorm2(block(b[j], geo, 0), nh, &b2[j]))) return rc;
+    if (!std::isfinite(b2[j])) return fail(QEXSTAG_ERR_NAN, "cgm_ee: source is not finite");
+  }
   int status = QEXSTAG_OK;
   double worst = 0.0;
-  for (int j = 0; j < nrhs; j++) {
-    double b2 = 0;
-    if ((rc = vnorm2(block(b[j], geo, 0), nh, &b2))) return rc;
-    if (!std::isfinite(b2)) return fail(QEXSTAG_ERR_NAN, "cgm_ee: source is not finite");
+  if (sloppy) {
+    // the right-hand sides of one shift together: a multi-right-hand-side
+    // FP32 CG (cgm_core with the one shift) on their FP64 residuals, y += d,
+    // repeated while any is above its target
+    std::vector<double2 *> rbuf(kMaxRhs), dbuf(kMaxRhs);
+    void *pt;
+    for (int j = 0; j < kMaxRhs; j++) {
+      void *a, *c;
+      if ((rc = g->ws.get(kSlotMs0 + 100 + j, vb, &a)) || (rc = g->ws.get(kSlotMs0 + 110 + j, vb, &c))) return rc;
+      rbuf[j] = (double2 *)a;
+      dbuf[j] = (double2 *)c;
+    }
+    if ((rc = g->ws.get(kSlotMs0 + 51, vb, &pt))) return rc;
+    double2 *t = (double2 *)pt;
+    const double zero = 0.0;
     for (int k = 0; k < nshift; k++) {
       const double m2s = m * m + 0.25 * sigma[k];
-      double2 *yk = y[j * nshift + k];
-      double r2 = 0;
-      if ((rc = shifted_residual(g, m2s, b[j], yk, r, t, &r2))) return rc;
-      const double r2stop = p->r2req * b2;
-      int pass = 0;
-      while (r2 > r2stop && pass < 10 && st->iterations < maxits) {
-        CgOut o{};
-        int rel = 0;
-        const int mx = maxits - st->iterations;
-        if (sloppy)
-          rc = cg_mixed(g, 0, m2s, CVecD{r, nh}, VecD{d, nh}, 0.5 * r2stop / r2, mx, p->sloppy,
-                        p->delta > 0 ? p->delta : (p->sloppy == QEXSTAG_SLOPPY_HALF ? 0.3 : 0.1), &o, &rel);
-        else
-          rc = cg64(g, 0, m2s, CVecD{r, nh}, VecD{d, nh}, 0.5 * r2stop / r2, mx, &o);
-        if (rc) return rc;
-        st->iterations += o.iterations;
-        st->reliable_updates += rel;
-        st->outer_iterations += 1;
-        if ((rc = vaxpy(block(yk, geo, 0), 1.0, CVecD{d, nh}, nh))) return rc;
-        if ((rc = shifted_residual(g, m2s, b[j], yk, r, t, &r2))) return rc;
-        pass++;
+      for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
+        const int nr = std::min(kMaxRhs, nrhs - j0);
+        std::vector<double> r2(nr);
+        for (int j = 0; j < nr; j++)
+          if ((rc = shifted_residual(g, m2s, b[j0 + j], y[(j0 + j) * nshift + k], rbuf[j], t, &r2[j]))) return rc;
+        for (int pass = 0; pass < 10 && st->iterations < maxits; pass++) {
+          // systems still above target, packed to the front
+          std::vector<int> live;
+          double req = 1.0;
+          for (int j = 0; j < nr; j++) {
+            const double stop = p->r2req * b2[j0 + j];
+            if (r2[j] > stop) {
+              live.push_back(j);
+              req = std::min(req, 0.5 * stop / r2[j]);
+            }
+          }
+          if (live.empty()) break;
+          req = std::max(req, 1e-12);  // what an FP32 inner solve can reach
+          const double2 *rb[kMaxRhs];
+          double2 *dy[kMaxRhs];
+          for (size_t q = 0; q < live.size(); q++) {
+            rb[q] = rbuf[live[q]];
+            dy[q] = dbuf[live[q]];
+          }
+          int its = 0;
+          if ((rc = cgm_core(g, 0, m2s, 1, &zero, (int)live.size(), rb, nh, dy, nh, 1.0, req,
+                             maxits - st->iterations, true, false, &its)))
+            return rc;
+          st->iterations += its;
+          st->outer_iterations += 1;
+          for (size_t q = 0; q < live.size(); q++) {
+            const int j = live[q];
+            double2 *yk = y[(j0 + j) * nshift + k];
+            if ((rc = vaxpy(block(yk, geo, 0), 1.0, CVecD{dbuf[j], nh}, nh)) ||
+                (rc = shifted_residual(g, m2s, b[j0 + j], yk, rbuf[j], t, &r2[j])))
+              return rc;
+          }
+        }
+        for (int j = 0; j < nr; j++) {
+          const double rel2 = b2[j0 + j] > 0 ? r2[j] / b2[j0 + j] : 0.0;
+          if (r2_out) r2_out[(j0 + j) * nshift + k] = rel2;
+          worst = std::max(worst, rel2);
+          if (r2[j] > p->r2req * b2[j0 + j]) status = QEXSTAG_NOT_CONVERGED;
+        }
       }
-      const double rel2 = b2 > 0 ? r2 / b2 : 0.0;
-      if (r2_out) r2_out[j * nshift + k] = rel2;
-      worst = std::max(worst, rel2);
-      if (r2 > r2stop) status = QEXSTAG_NOT_CONVERGED;
+    }
+  } else {
+    void *pr, *pt, *pd;
+    if ((rc = g->ws.get(kSlotMs0 + 50, vb, &pr)) || (rc = g->ws.get(kSlotMs0 + 51, vb, &pt)) ||
+        (rc = g->ws.get(kSlotMs0 + 52, vb, &pd)))
+      return rc;
+    double2 *r = (double2 *)pr, *t = (double2 *)pt, *d = (double2 *)pd;
+    for (int j = 0; j < nrhs; j++) {
+      for (int k = 0; k < nshift; k++) {
+        const double m2s = m * m + 0.25 * sigma[k];
+        double2 *yk = y[j * nshift + k];
+        double r2 = 0;
+        if ((rc = shifted_residual(g, m2s, b[j], yk, r, t, &r2))) return rc;
+        const double r2stop = p->r2req * b2[j];
+        int pass = 0;
+        while (r2 > r2stop && pass < 10 && st->iterations < maxits) {
+          CgOut o{};
+          const int mx = maxits - st->iterations;
+          if ((rc = cg64(g, 0, m2s, CVecD{r, nh}, VecD{d, nh}, 0.5 * r2stop / r2, mx, &o))) return rc;
+          st->iterations += o.iterations;
+          st->outer_iterations += 1;
+          if ((rc = vaxpy(block(yk, geo, 0), 1.0, CVecD{d, nh}, nh))) return rc;
+          if ((rc = shifted_residual(g, m2s, b[j], yk, r, t, &r2))) return rc;
+          pass++;
+        }
+        const double rel2 = b2[j] > 0 ? r2 / b2[j] : 0.0;
+        if (r2_out) r2_out[j * nshift + k] = rel2;
+        worst = std::max(worst, rel2);
+        if (r2 > r2stop) status = QEXSTAG_NOT_CONVERGED;
+      }
     }
   }
   st->r2 = worst;
