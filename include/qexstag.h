@@ -256,6 +256,14 @@ int qexstag_force_solve(qexstag_links *g, double *psi, const double *phi, double
    consumes.  Layout as qexstag_force's f. */
 int qexstag_ferm_outer(qexstag_links *g, double *f, const double *psi, int mem);
 
+/* Self-test of the batched solver's grid barrier (the one wait inside a
+   library kernel): a cooperative kernel of one block per SM passes the
+   barrier twice, each wait limited to timeout_ms.  With missing = 0 it
+   returns QEXSTAG_OK; with missing > 0 the barrier waits for that many
+   blocks that never arrive, every block gives up after timeout_ms, and the
+   call returns QEXSTAG_ERR_TIMEOUT with the device still usable. */
+int qexstag_barrier_selftest(int missing, double timeout_ms);
+
 /* ---- HISQ link smearing (src/gauge/fat7l.nim, src/physics/hisqLinks.nim,
    src/gauge/hisqsmear.nim) ----
    Gauge fields here are the four directions of a link field:

@@ -155,6 +155,7 @@ SIGNATURES = {
     "qexstag_domain_links": (I, [PP, I, PP, I]),
     "qexstag_domain_stagD2ee": (I, [PP, I, PP, PP, D, I]),
     "qexstag_domain_solveEE": (I, [PP, I, PP, PP, D, P, P, I]),
+    "qexstag_barrier_selftest": (I, [I, D]),
 }
 
 _lib = None

@@ -81,15 +81,17 @@ __device__ __forceinline__ int ld_int(const int *p) { return *(volatile const in
 __device__ __forceinline__ double ld_dbl(const double *p) { return __ldcg(p); }
 
 // Grid barrier with a time limit; returns false (in every thread) when the
-// barrier failed or another block reported an error.
-__device__ bool grid_sync(BGlobal *gl, long long timeout) {
+// barrier failed or another block reported an error.  missing > 0 makes the
+// barrier wait for that many blocks that do not exist (the self-test's
+// stand-in for a block that never arrives).
+__device__ bool grid_sync(BGlobal *gl, long long timeout, unsigned missing = 0) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned gen = *(volatile unsigned *)&gl->bar_gen;
     __threadfence();
     const unsigned arrived = atomicAdd(&gl->bar_count, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == gridDim.x - 1 + missing) {
       gl->bar_count = 0;
       __threadfence();
       atomicAdd(&gl->bar_gen, 1u);
@@ -109,6 +111,13 @@ __device__ bool grid_sync(BGlobal *gl, long long timeout) {
   }
   __syncthreads();
   return ok;
+}
+
+// every block passes the barrier twice; out = 1 when both passed
+__global__ void barrier_selftest_kernel(BGlobal *gl, long long timeout, unsigned missing, int *out) {
+  const bool a = grid_sync(gl, timeout, missing);
+  const bool b = a && grid_sync(gl, timeout, missing);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *out = (a && b) ? 1 : 0;
 }
 
 __device__ __forceinline__ int find_prob(const int *offs, int n, int s) {
@@ -727,3 +736,50 @@ int solve_batched(int nprob, qexstag_links_s *const *gs, const double *mass, dou
 }
 
 }  // namespace qs
+
+using namespace qs;
+
+extern "C" {
+
+int qexstag_barrier_selftest(int missing, double timeout_ms) {
+  if (missing < 0 || missing > 1024 || !(timeout_ms > 0.0) || timeout_ms > 10000.0)
+    return fail(QEXSTAG_ERR_ARG, "barrier_selftest: missing in [0, 1024], timeout in (0, 10000] ms");
+  int rc = runtime_ready();
+  if (rc) return rc;
+  int dev = 0, khz = 0;
+  QS_CUDA(cudaGetDevice(&dev));
+  QS_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+  const long long cycles = (long long)(timeout_ms * (double)khz);  // kHz x ms = cycles
+  BGlobal *gl = nullptr;
+  int *out = nullptr;
+  if (cudaMalloc(&gl, sizeof(BGlobal)) != cudaSuccess || cudaMalloc(&out, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    if (gl) cudaFree(gl);
+    return fail(QEXSTAG_ERR_ALLOC, "barrier_selftest: allocation failed");
+  }
+  QS_CUDA(cudaMemsetAsync(gl, 0, sizeof(BGlobal), stream()));
+  QS_CUDA(cudaMemsetAsync(out, 0, sizeof(int), stream()));
+  // one block per SM: always co-resident, as the cooperative launch checks
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(num_sms());
+  cfg.blockDim = dim3(128);
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, barrier_selftest_kernel, gl, cycles, (unsigned)missing, out);
+  note_launch();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream());
+  int hout = 0, herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&hout, out, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&herr, &gl->err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(gl);
+  cudaFree(out);
+  if (e != cudaSuccess) return cuda_fail(e, "barrier_selftest");
+  if (herr || hout != 1) return fail(QEXSTAG_ERR_TIMEOUT, "barrier_selftest: the grid barrier timed out");
+  return QEXSTAG_OK;
+}
+
+}  // extern "C"

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from qex_b200 import _lib as L
 from qex_b200 import fields as F
 from qex_b200 import stag as S
 
@@ -74,3 +75,29 @@ def test_batched_rejects_bad_input(cuda):
     with pytest.raises(S.L.QexStagError):
         S.solve_batched(stags, xs, [b for *_, b in probs], [0.1, 0.1],
                         S.SolverParams(r2req=1e-20, sloppySolve=S.L.SLOPPY_HALF))
+
+
+def test_barrier_timeout_is_reported(cuda):
+    """Failure detection without a GPU fault: the batched solver's grid
+    barrier waits for a block that never arrives, gives up after its time
+    limit, and the call reports QEXSTAG_ERR_TIMEOUT; the context stays
+    usable (the barrier and a solve run afterwards)."""
+    import time
+    lib = L.load()
+    assert lib.qexstag_barrier_selftest(0, 1000.0) == L.OK
+    t0 = time.perf_counter()
+    rc = lib.qexstag_barrier_selftest(1, 50.0)
+    dt = time.perf_counter() - t0
+    assert rc == L.ERR_TIMEOUT, rc
+    assert "timed out" in lib.qexstag_last_error().decode()
+    assert dt < 5.0, dt
+    assert lib.qexstag_barrier_selftest(0, 1000.0) == L.OK
+    assert lib.qexstag_barrier_selftest(-1, 50.0) == L.ERR_ARG
+    dims = (4, 4, 4, 4)
+    g = F.naive_links(dims, 0.3, 2)
+    s = S.Staggered(S.Layout(dims), g)
+    b = F.even_source(dims, 3)
+    x = np.zeros_like(b)
+    sp = S.SolverParams(r2req=1e-20)
+    s.solveEE(x, b, 0.1, sp)
+    assert sp.status == L.OK
