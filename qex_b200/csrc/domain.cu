@@ -18,12 +18,24 @@
 // Neighbours held by the same process (several ranks on one device) are
 // exchanged by device-to-device copies; neighbours in other processes by
 // NCCL send/receive of the boundary slices into the receiver's ghost slices
-// and an NCCL all-reduce of the partial sums.  NCCL is resolved at run time
+// and an NCCL all-reduce of the partial sums.  The exchange runs on a side
+// stream while the sweeps that need no ghost run on the library's stream:
+// with reach rho (3 with Naik links, 1 without; h = 2 rho) the odd
+// intermediate on slices [h+rho, h+T-rho) and the even output on
+// [h+2rho, h+T-2rho) read interior slices only; the 2 rho slices at each
+// end of both sweeps follow the exchange.
+//
+// The CG keeps its scalars on the device (the CgState of the one-lattice
+// CG): each domain's interior partial sum goes to a slot, one thread adds
+// the slots in rank order, NCCL all-reduces that value in place, and the
+// next kernel finishes alpha or beta, so an iteration makes no host round
+// trip and the host reads the state every few iterations.  NCCL is resolved at run time
 // from the libnccl.so.2 already loaded in the process (the one torch
 // carries) or the system's, so the library does not link a second copy.
 #include <dlfcn.h>
 #include <nccl.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -91,7 +103,9 @@ struct qexstag_domain_s {
   ncclComm_t comm = nullptr;        // inter-process neighbours
   bool connected = false;
   std::vector<qs::Geom> local;      // geometry of the T-slice local lattice
-  double *dsum = nullptr;           // device scalar for all-reduce
+  double *dsum = nullptr;           // device scalars: see DevScalars
+  cudaStream_t side = nullptr;      // ghost exchange, overlapped with the interior
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace qs {
@@ -101,13 +115,25 @@ enum DomainSlot {
   kDmIn = kSlotLast + 700, kDmOut, kDmT, kDmFull, kDmX, kDmR, kDmP, kDmAp, kDmSoa, kDmLinks
 };
 
+// layout of a domain's device scalars (dsum): the partial sums of up to
+// kMaxSet domains of one call, the combined value, then the CG state
+constexpr int kMaxSet = 64;
+constexpr int kValOff = kMaxSet;
+constexpr int kStateOff = kMaxSet + 8;
+constexpr size_t kDevScalarBytes = sizeof(double) * kStateOff + sizeof(CgState);
+
+int read_state(const CgState *dst, CgState *host);
+int write_state(CgState *dst, const CgState &host);
+int check_interval(int nh);
+
 static size_t slice_half(const qexstag_domain_s *d) {
   return (size_t)d->gdims[0] * d->gdims[1] * d->gdims[2] / 2;
 }
 
 // one parity block's ghost exchange of ncomp component arrays, each with
 // stride V_ext, of the fields at base[k] of each domain of the set
-static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, int ncomp, int par) {
+static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, int ncomp, int par,
+                    cudaStream_t s) {
   const size_t sh = slice_half(ds[0]);
   for (int k = 0; k < n; k++) {
     qexstag_domain_s *d = ds[k];
@@ -119,10 +145,10 @@ static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, in
       for (int c = 0; c < ncomp; c++) {
         double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
         // my top interior slices -> up's lower ghosts; my bottom -> down's upper
-        QS_NCCL(nccl().send(f + (size_t)d->T * sh, 2 * cnt, ncclDouble, upr, d->comm, stream()));
-        QS_NCCL(nccl().recv(f, 2 * cnt, ncclDouble, dnr, d->comm, stream()));
-        QS_NCCL(nccl().send(f + (size_t)d->h * sh, 2 * cnt, ncclDouble, dnr, d->comm, stream()));
-        QS_NCCL(nccl().recv(f + (size_t)(d->h + d->T) * sh, 2 * cnt, ncclDouble, upr, d->comm, stream()));
+        QS_NCCL(nccl().send(f + (size_t)d->T * sh, 2 * cnt, ncclDouble, upr, d->comm, s));
+        QS_NCCL(nccl().recv(f, 2 * cnt, ncclDouble, dnr, d->comm, s));
+        QS_NCCL(nccl().send(f + (size_t)d->h * sh, 2 * cnt, ncclDouble, dnr, d->comm, s));
+        QS_NCCL(nccl().recv(f + (size_t)(d->h + d->T) * sh, 2 * cnt, ncclDouble, upr, d->comm, s));
       }
       QS_NCCL(nccl().groupEnd());
     } else {
@@ -137,10 +163,9 @@ static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, in
         double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
         const double2 *fd = base[kd] + (size_t)c * V + (size_t)par * nh;
         const double2 *fu = base[ku] + (size_t)c * V + (size_t)par * nh;
-        QS_CUDA(cudaMemcpyAsync(f, fd + (size_t)d->down->T * sh, cnt * sizeof(double2), cudaMemcpyDeviceToDevice,
-                                stream()));
+        QS_CUDA(cudaMemcpyAsync(f, fd + (size_t)d->down->T * sh, cnt * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         QS_CUDA(cudaMemcpyAsync(f + (size_t)(d->h + d->T) * sh, fu + (size_t)d->up->h * sh, cnt * sizeof(double2),
-                                cudaMemcpyDeviceToDevice, stream()));
+                                cudaMemcpyDeviceToDevice, s));
       }
     }
   }
@@ -212,6 +237,8 @@ static int check_set(qexstag_domain_s *const *ds, int n) {
     if ((ds[k]->comm != nullptr) != (ds[0]->comm != nullptr))
       return fail(QEXSTAG_ERR_ARG, "domain: in-process and NCCL domains in one call");
   }
+  if (n > kMaxSet) return fail(QEXSTAG_ERR_ARG, "domain: more than 64 domains in one call");
+  if (ds[0]->comm && n > 1) return fail(QEXSTAG_ERR_ARG, "domain: one NCCL-connected domain per call");
   return runtime_ready();
 }
 
@@ -269,15 +296,50 @@ static VecD interior(qexstag_domain_s *d, double2 *f) {
 }
 static int interior_n(qexstag_domain_s *d) { return (int)(d->T * slice_half(d)); }
 
-// r = stagD2ee(m2) x on every domain: one exchange of x, then the Schur
-// kernels on the extended lattice
+// r = stagD2ee(m2) x on every domain (even interior sites; t is the odd
+// block of the intermediate).  The ghost exchange of x runs on the side
+// stream while the sweeps that read interior slices only run on the
+// library's stream; the slices next to the ghosts follow the exchange.
+// Skipped once *done is set (the exchange still runs, unread).
 static int schur_set(qexstag_domain_s *const *ds, int n, double2 *const *r, double2 *const *x, double2 *const *t,
-                     double m2) {
+                     double m2, const int *done = nullptr) {
   int rc;
-  if ((rc = exchange(ds, n, x, 3, 0))) return rc;
+  qexstag_domain_s *d0 = ds[0];
+  const int sh = (int)slice_half(d0), h = d0->h, T = d0->T;
+  const int rho = h / 2;                 // reach of the longest hop
+  const bool overlap = T > 4 * rho;      // some slices need no ghost at all
+  QS_CUDA(cudaEventRecord(d0->fork, stream()));
+  QS_CUDA(cudaStreamWaitEvent(d0->side, d0->fork, 0));
+  if ((rc = exchange(ds, n, x, 3, 0, d0->side))) return rc;
+  QS_CUDA(cudaEventRecord(d0->join, d0->side));
+  for (int k = 0; overlap && k < n; k++) {
+    const Geom &g = ds[k]->ext->g;
+    const CVecD xe{x[k], g.V}, te{t[k] + g.nh, g.V};
+    // t = (2D)_oe x on [h+rho, h+T-rho), r = 4 m2 x - (2D)_eo t on [h+2rho, h+T-2rho)
+    if ((rc = dslash64_ranges(ds[k]->g, 1, VecD{t[k] + g.nh, g.V}, xe, CVecD{nullptr, 0}, 0.0, 1.0, +1,
+                              (h + rho) * sh, (h + T - rho) * sh, 0, 0, done)) ||
+        (rc = dslash64_ranges(ds[k]->g, 0, VecD{r[k], g.V}, te, xe, 4.0 * m2, 1.0, -1, (h + 2 * rho) * sh,
+                              (h + T - 2 * rho) * sh, 0, 0, done)))
+      return rc;
+  }
+  QS_CUDA(cudaStreamWaitEvent(stream(), d0->join, 0));
   for (int k = 0; k < n; k++) {
     const Geom &g = ds[k]->ext->g;
-    if ((rc = schur64(ds[k]->g, 0, VecD{r[k], g.V}, CVecD{x[k], g.V}, VecD{t[k] + g.nh, g.V}, m2))) return rc;
+    const CVecD xe{x[k], g.V}, te{t[k] + g.nh, g.V};
+    if (overlap) {
+      rc = dslash64_ranges(ds[k]->g, 1, VecD{t[k] + g.nh, g.V}, xe, CVecD{nullptr, 0}, 0.0, 1.0, +1,
+                           (h - rho) * sh, (h + rho) * sh, (h + T - rho) * sh, (h + T + rho) * sh, done);
+      if (!rc)
+        rc = dslash64_ranges(ds[k]->g, 0, VecD{r[k], g.V}, te, xe, 4.0 * m2, 1.0, -1, h * sh, (h + 2 * rho) * sh,
+                             (h + T - 2 * rho) * sh, (h + T) * sh, done);
+    } else {
+      rc = dslash64_ranges(ds[k]->g, 1, VecD{t[k] + g.nh, g.V}, xe, CVecD{nullptr, 0}, 0.0, 1.0, +1,
+                           (h - rho) * sh, (h + T + rho) * sh, 0, 0, done);
+      if (!rc)
+        rc = dslash64_ranges(ds[k]->g, 0, VecD{r[k], g.V}, te, xe, 4.0 * m2, 1.0, -1, h * sh, (h + T) * sh, 0, 0,
+                             done);
+    }
+    if (rc) return rc;
   }
   return QEXSTAG_OK;
 }
@@ -294,6 +356,147 @@ static int dot_set(qexstag_domain_s *const *ds, int n, double2 *const *a, double
     if (rc) return rc;
   }
   return allreduce_sum(ds, n, v.data(), out);
+}
+
+// ---- device-resident CG over the domains ----
+
+__global__ void __launch_bounds__(kBlock)
+    dm_p_kernel(const double2 *__restrict__ r, double2 *__restrict__ p, int stride, int n, const CgState *st) {
+  if (st->done) return;
+  const bool first = (st->itn == 0);
+  const double beta = st->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 rv = r[(size_t)c * stride + i];
+      if (first) {
+        p[(size_t)c * stride + i] = rv;
+      } else {
+        const double2 pv = p[(size_t)c * stride + i];
+        p[(size_t)c * stride + i] = make_double2(fma(beta, pv.x, rv.x), fma(beta, pv.y, rv.y));
+      }
+    }
+  }
+}
+
+// Re <a, b> over one domain's interior into *slot
+__global__ void __launch_bounds__(kBlock)
+    dm_dot_kernel(const double2 *__restrict__ a, const double2 *__restrict__ b, int stride, int n,
+                  const CgState *st, double *slot, double *partials, unsigned *ticket) {
+  if (st->done) return;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 u = a[(size_t)c * stride + i], v = b[(size_t)c * stride + i];
+      s = fma(u.x, v.x, s);
+      s = fma(u.y, v.y, s);
+    }
+  }
+  double v[1] = {s}, o[1];
+  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) *slot = o[0];
+}
+
+// x += alpha p, r -= alpha Ap on one domain's interior; |r|^2 into *slot
+__global__ void __launch_bounds__(kBlock)
+    dm_xr_kernel(double2 *__restrict__ x, double2 *__restrict__ r, const double2 *__restrict__ p,
+                 const double2 *__restrict__ ap, int stride, int n, const CgState *st, double *slot,
+                 double *partials, unsigned *ticket) {
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const size_t o = (size_t)c * stride + i;
+      const double2 pv = p[o], av = ap[o];
+      double2 xv = x[o], rv = r[o];
+      xv.x = fma(alpha, pv.x, xv.x);
+      xv.y = fma(alpha, pv.y, xv.y);
+      rv.x = fma(-alpha, av.x, rv.x);
+      rv.y = fma(-alpha, av.y, rv.y);
+      x[o] = xv;
+      r[o] = rv;
+      s = fma(rv.x, rv.x, s);
+      s = fma(rv.y, rv.y, s);
+    }
+  }
+  double v[1] = {s}, o[1];
+  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) *slot = o[0];
+}
+
+// One thread: the n slots added in rank order into *val (n = 0: *val as
+// the all-reduce left it), then what = 1: pAp, alpha = rz/pAp, itn += 1;
+// what = 2: r2, beta = r2/rz, done (cg.nim:213-240).
+__global__ void dm_scalar_kernel(const double *slots, int n, double *val, CgState *st, int what) {
+  if (st->done) return;
+  double s;
+  if (n > 0) {
+    s = 0.0;
+    for (int k = 0; k < n; k++) s += slots[k];
+    *val = s;
+  } else {
+    s = *val;
+  }
+  if (what == 1) {
+    st->pAp = s;
+    st->alpha = st->rz / s;
+    st->itn += 1;
+  } else if (what == 2) {
+    st->r2 = s;
+    st->beta = s / st->rz;
+    st->rz = s;
+    if (isnan(s)) st->nan = 1;
+    st->done = (!(st->itn < st->maxits && s > st->r2stop) || st->nan) ? 1 : 0;
+  }
+}
+
+static int finish_scalar(qexstag_domain_s *const *ds, int n, CgState *st, int what) {
+  double *slots = ds[0]->dsum, *val = ds[0]->dsum + kValOff;
+  if (ds[0]->comm) {
+    dm_scalar_kernel<<<1, 1, 0, stream()>>>(slots, n, val, st, 0);
+    QS_NCCL(nccl().allReduce(val, val, 1, ncclDouble, ncclSum, ds[0]->comm, stream()));
+    dm_scalar_kernel<<<1, 1, 0, stream()>>>(nullptr, 0, val, st, what);
+    note_launch(2);
+  } else {
+    dm_scalar_kernel<<<1, 1, 0, stream()>>>(slots, n, val, st, what);
+    note_launch();
+  }
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
+// one CG iteration (cg.nim:174-240, cpNone) enqueued without a host sync
+static int cg_iteration(qexstag_domain_s *const *ds, int n, double2 *const *xv, double2 *const *rv,
+                        double2 *const *pv, double2 *const *ap, double2 *const *tv, double m2, CgState *st) {
+  int rc;
+  for (int k = 0; k < n; k++) {
+    const int ni = interior_n(ds[k]);
+    const VecD r = interior(ds[k], rv[k]), p = interior(ds[k], pv[k]);
+    dm_p_kernel<<<grid_for(ni), kBlock, 0, stream()>>>(r.p, p.p, p.stride, ni, st);
+  }
+  note_launch(n);
+  QS_LAUNCH_CHECK();
+  if ((rc = schur_set(ds, n, ap, pv, tv, m2, &st->done))) return rc;
+  for (int k = 0; k < n; k++) {
+    const int ni = interior_n(ds[k]);
+    const VecD p = interior(ds[k], pv[k]), a = interior(ds[k], ap[k]);
+    dm_dot_kernel<<<std::min(grid_for(ni), kMaxRedBlocks), kBlock, 0, stream()>>>(
+        p.p, a.p, p.stride, ni, st, ds[0]->dsum + k, red_partials(), red_tickets());
+  }
+  note_launch(n);
+  QS_LAUNCH_CHECK();
+  if ((rc = finish_scalar(ds, n, st, 1))) return rc;
+  for (int k = 0; k < n; k++) {
+    const int ni = interior_n(ds[k]);
+    const VecD x = interior(ds[k], xv[k]), r = interior(ds[k], rv[k]), p = interior(ds[k], pv[k]),
+               a = interior(ds[k], ap[k]);
+    dm_xr_kernel<<<std::min(grid_for(ni), kMaxRedBlocks), kBlock, 0, stream()>>>(
+        x.p, r.p, p.p, a.p, p.stride, ni, st, ds[0]->dsum + k, red_partials(), red_tickets());
+  }
+  note_launch(n);
+  QS_LAUNCH_CHECK();
+  return finish_scalar(ds, n, st, 2);
 }
 
 }  // namespace qs
@@ -335,9 +538,15 @@ int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nl
   qexstag_layout_destroy(ll);
   void *z = nullptr;
   const size_t lb = sizeof(double2) * 9 * (size_t)le->g.V * nlinks;
-  if (cudaMalloc(&z, lb) != cudaSuccess || cudaMalloc((void **)&d->dsum, sizeof(double)) != cudaSuccess) {
+  if (cudaMalloc(&z, lb) != cudaSuccess || cudaMalloc((void **)&d->dsum, kDevScalarBytes) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->join, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     if (z) cudaFree(z);
+    if (d->dsum) cudaFree(d->dsum);
+    if (d->side) cudaStreamDestroy(d->side);
+    if (d->fork) cudaEventDestroy(d->fork);
     qexstag_layout_destroy(le);
     delete d;
     return fail(QEXSTAG_ERR_ALLOC, "domain_create: device allocation failed");
@@ -351,6 +560,9 @@ int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nl
   cudaFree(z);
   if (rc) {
     cudaFree(d->dsum);
+    cudaStreamDestroy(d->side);
+    cudaEventDestroy(d->fork);
+    cudaEventDestroy(d->join);
     qexstag_layout_destroy(le);
     delete d;
     return rc;
@@ -365,6 +577,12 @@ int qexstag_domain_destroy(qexstag_domain *d) {
   if (d->g) qexstag_links_destroy(d->g);
   if (d->ext) qexstag_layout_destroy(d->ext);
   if (d->dsum) cudaFree(d->dsum);
+  if (d->side) {
+    cudaStreamSynchronize(d->side);
+    cudaStreamDestroy(d->side);
+  }
+  if (d->fork) cudaEventDestroy(d->fork);
+  if (d->join) cudaEventDestroy(d->join);
   delete d;
   return QEXSTAG_OK;
 }
@@ -441,7 +659,7 @@ int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const
   // ghosts of every link component, both parities
   const int ncomp = 9 * doms[0]->nl;
   for (int par = 0; par < 2; par++)
-    if ((rc = exchange(doms, n, base.data(), ncomp, par))) return rc;
+    if ((rc = exchange(doms, n, base.data(), ncomp, par, stream()))) return rc;
   QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
 }
@@ -505,40 +723,31 @@ int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x,
         (rc = vcopy(interior(d, pv[k]), cv(interior(d, bv[k])), ni)))
       return rc;
   }
-  double b2 = 0, r2 = 0, pAp = 0;
+  double b2 = 0;
   if ((rc = dot_set(doms, n, bv.data(), bv.data(), &b2))) return rc;
   if (!std::isfinite(b2)) return fail(QEXSTAG_ERR_NAN, "domain_solveEE: source is not finite");
-  r2 = b2;
   const double r2stop = p->r2req * b2;
   const int maxits = p->maxits > 0 ? p->maxits : 50000;
-  int its = 0;
+  CgState hs;
+  std::memset(&hs, 0, sizeof hs);
+  hs.b2 = hs.r2 = hs.rz = b2;
+  hs.r2req = p->r2req;
+  hs.r2stop = r2stop;
+  hs.maxits = maxits;
+  hs.done = (b2 > r2stop) ? 0 : 1;
+  CgState *st = (CgState *)(doms[0]->dsum + kStateOff);
+  if ((rc = write_state(st, hs))) return rc;
+  int total = 0;
+  for (int k = 0; k < n; k++) total += interior_n(doms[k]);
+  const int every = check_interval(total);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, stream());
-  while (r2 > r2stop && its < maxits) {
-    if ((rc = schur_set(doms, n, ap.data(), pv.data(), tv.data(), m2))) break;
-    if ((rc = dot_set(doms, n, pv.data(), ap.data(), &pAp))) break;
-    const double alpha = r2 / pAp;
-    for (int k = 0; k < n && !rc; k++) {
-      qexstag_domain_s *d = doms[k];
-      const int ni = interior_n(d);
-      rc = vaxpy(interior(d, xv[k]), alpha, cv(interior(d, pv[k])), ni);
-      if (!rc) rc = vaxpy(interior(d, rv[k]), -alpha, cv(interior(d, ap[k])), ni);
-    }
-    if (rc) break;
-    double r2n;
-    if ((rc = dot_set(doms, n, rv.data(), rv.data(), &r2n))) break;
-    if (!std::isfinite(r2n)) {
-      rc = fail(QEXSTAG_ERR_NAN, "domain_solveEE: NaN residual");
-      break;
-    }
-    const double beta = r2n / r2;
-    r2 = r2n;
-    its++;
-    for (int k = 0; k < n && !rc; k++)
-      rc = vxpay(interior(doms[k], pv[k]), cv(interior(doms[k], rv[k])), beta, interior_n(doms[k]));
-    if (rc) break;
+  while (!hs.done) {
+    for (int i = 0; i < every && !rc; i++) rc = cg_iteration(doms, n, xv.data(), rv.data(), pv.data(), ap.data(),
+                                                            tv.data(), m2, st);
+    if (rc || (rc = read_state(st, &hs))) break;
   }
   cudaEventRecord(e1, stream());
   cudaEventSynchronize(e1);
@@ -546,6 +755,8 @@ int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x,
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  const int its = hs.itn;
+  if (!rc && hs.nan) rc = fail(QEXSTAG_ERR_NAN, "domain_solveEE: NaN residual");
   if (rc) return rc;
   // true residual
   for (int k = 0; k < n; k++) {

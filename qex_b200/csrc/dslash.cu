@@ -38,6 +38,9 @@ struct DslashArgs64 {
   double *partials;
   unsigned *ticket;
   double *dot_out;
+  // output sites: [k0, k0 + n1) then [k2, k2 + nsites - n1) of the parity
+  // block (the whole block: k0 = k2 = 0, n1 = nsites = nh)
+  int k0, n1, k2, nsites;
 };
 
 template <int NL, int HOP, int INIT, int RED>
@@ -50,7 +53,8 @@ __global__ void __launch_bounds__(kBlock) dslash64_kernel(const DslashArgs64 A) 
   const size_t in_base = (size_t)(1 - A.po) * nh;
   const size_t out_base = (size_t)A.po * nh;
   double dot = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < A.nsites; j += gridDim.x * blockDim.x) {
+    const int k = j < A.n1 ? A.k0 + j : A.k2 + (j - A.n1);
     int x[4], lex;
     site_coords(g, A.po, k, x, lex);
     double2 acc[3];
@@ -191,10 +195,49 @@ int dslash64(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, C
   A.partials = red_partials();
   A.ticket = red_tickets();
   A.dot_out = dot_out;
+  A.k0 = A.k2 = 0;
+  A.n1 = A.nsites = g.nh;
   int grid = grid_for(g.nh, kBlock, 6);
   if (red != kRedNone && grid > kMaxRedBlocks) grid = kMaxRedBlocks;
   int rc = (gl->nl == 8) ? dispatch64<8>(A, hop, init, red, grid)
                          : dispatch64<4>(A, hop, init, red, grid);
+  if (rc) return rc;
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
+// One half sweep over the sites [k0, k1) and [k2, k3) of parity po (either
+// range may be empty): out = b xs + c (2D) xin with hop sign hop, no
+// reduction; skipped once *done is set.  Used for the halo-overlapped
+// Schur operator of a domain, whose interior sweeps run while the ghost
+// slices are in flight.
+int dslash64_ranges(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, double b, double c,
+                    int hop, int k0, int k1, int k2, int k3, const int *done) {
+  const Geom &g = gl->l->g;
+  if (k0 < 0 || k1 < k0 || k2 < 0 || k3 < k2 || k1 > g.nh || k3 > g.nh)
+    return fail(QEXSTAG_ERR_ARG, "dslash64_ranges: site range outside the parity block");
+  DslashArgs64 A;
+  std::memset(&A, 0, sizeof(A));
+  A.g = g;
+  A.po = po;
+  A.u = gl->u64;
+  A.xin = xin.p;
+  A.istride = xin.stride;
+  A.xs = xs.p;
+  A.sstride = xs.stride;
+  A.out = out.p;
+  A.ostride = out.stride;
+  A.b = b;
+  A.c = c;
+  A.done = done;
+  A.k0 = k0;
+  A.n1 = k1 - k0;
+  A.k2 = k2;
+  A.nsites = (k1 - k0) + (k3 - k2);
+  if (A.nsites == 0) return QEXSTAG_OK;
+  const int init = xs.p ? 1 : 0;
+  const int rc = (gl->nl == 8) ? dispatch64<8>(A, hop, init, kRedNone, grid_for(A.nsites, kBlock, 6))
+                               : dispatch64<4>(A, hop, init, kRedNone, grid_for(A.nsites, kBlock, 6));
   if (rc) return rc;
   QS_LAUNCH_CHECK();
   return QEXSTAG_OK;
@@ -224,6 +267,7 @@ int schur64_plain(const qexstag_links_s *gl, int par, VecD r, CVecD x, VecD t, d
   std::memset(&A, 0, sizeof(A));
   A.g = g;
   A.u = gl->u64;
+  A.n1 = A.nsites = g.nh;
   const int grid = grid_for(g.nh, kBlock, 6);
   // t = (2D)_{q,par} x
   A.po = 1 - par;

@@ -82,6 +82,8 @@ int dslash64(const qexstag_links_s *g, int po, VecD out, CVecD xin, CVecD xs, CV
 int schur64(const qexstag_links_s *g, int par, VecD r, CVecD x, VecD t, double m2,
             int red = kRedNone, void *state = nullptr, const int *done = nullptr,
             double *dot_out = nullptr);
+int dslash64_ranges(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, double b, double c,
+                    int hop, int k0, int k1, int k2, int k3, const int *done);
 
 // ---- blas.cu ----
 int aos_to_soa(const double *aos, double2 *soa, int n, int stride, int ncomp);

@@ -108,3 +108,44 @@ def nccl_unique_id() -> bytes:
     buf = C.create_string_buffer(128)
     L.check(L.load().qexstag_nccl_unique_id(buf), "nccl_unique_id")
     return buf.raw
+
+
+def main():
+    """Device seconds of the FP64 domain CG for stagD2ee(m^2) y = b at --dims
+    (fat + Naik fields and source as the 32^4 benchmark's, m = 0.01,
+    r2req = 1e-20) with R ranks held by this process on one device, for each
+    R in --ranks, beside the one-lattice FP64 CG on the same problem."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dims", default="32,32,32,32")
+    ap.add_argument("--ranks", default="1,2")
+    ap.add_argument("--mass", type=float, default=0.01)
+    ap.add_argument("--r2req", type=float, default=1e-20)
+    a = ap.parse_args()
+    dims = tuple(int(v) for v in a.dims.split(","))
+    S.init(0)
+    g = F.fat_naik_links(dims, 21)
+    b = F.even_source(dims, 31)
+    one = S.Staggered(S.Layout(dims), g)
+    x = np.zeros_like(b)
+    sp = S.SolverParams(r2req=a.r2req)
+    one.solveEE(x, b, a.mass, sp)  # warm-up
+    sp = S.SolverParams(r2req=a.r2req)
+    one.solveEE(x, b, a.mass, sp)
+    out = {"dims": dims, "mass": a.mass, "one_lattice": {"iterations": sp.iterations, "seconds": sp.seconds}}
+    for R in (int(v) for v in a.ranks.split(",")):
+        d = DomainSet(dims, R, 8)
+        d.set_links(g)
+        for _ in range(2):  # warm-up, then the timed solve
+            y = np.zeros_like(b)
+            sp = S.SolverParams(r2req=a.r2req)
+            d.solveEE(y, b, a.mass, sp)
+        out[f"ranks_{R}"] = {"slab": d.ldims[3], "iterations": sp.iterations, "seconds": sp.seconds,
+                             "true_r2": sp.r2, "max_diff_vs_one_lattice": float(np.abs(y - x).max())}
+        del d
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
