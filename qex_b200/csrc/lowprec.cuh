@@ -187,6 +187,81 @@ __device__ __forceinline__ void store_vec(void *base, int stride, int i, const f
   }
 }
 
+// ---- packed-pair forms for the 16-bit Dslash (sm_100 FP32x2 instructions) ----
+//
+// The colour sums there are built as t_i = T_i + i S_i with
+// T_i = sum_j u_ij * Re v_j and S_i = sum_j u_ij * Im v_j, each term one
+// FP32x2 FMA of the link element's (re, im) pair with a vector component
+// broadcast to both lanes.
+
+// raw integers of a packed 16-bit pair as (sx re, sy im): exact, one FP32x2
+// op after the two byte permutes (sx, sy = +-1 fold a negation or a
+// conjugation into the decode)
+template <int SX, int SY>
+__device__ __forceinline__ float2 h2f2(unsigned w) {
+  constexpr float B = 8421376.0f;  // 2^23 + 32768
+  const float2 r = make_float2(__uint_as_float(__byte_perm(w, 0x4B00u, 0x5410)),
+                               __uint_as_float(__byte_perm(w, 0x4B00u, 0x5432)));
+  if (SX == 1 && SY == 1) return __fadd2_rn(r, make_float2(-B, -B));
+  return __ffma2_rn(r, make_float2((float)SX, (float)SY), make_float2(-SX * B, -SY * B));
+}
+
+// 18-real 16-bit link f at site as (re, im) pairs, times (SX, SY) per pair
+template <int SX, int SY>
+__device__ __forceinline__ void load_link18_x2(const uint4 *c16, const unsigned *t16, int f, size_t site,
+                                               size_t V, float2 u[9]) {
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const uint4 q = ldlink(c16 + ((size_t)f * 2 + j) * V + site);
+    u[4 * j] = h2f2<SX, SY>(q.x);
+    u[4 * j + 1] = h2f2<SX, SY>(q.y);
+    u[4 * j + 2] = h2f2<SX, SY>(q.z);
+    u[4 * j + 3] = h2f2<SX, SY>(q.w);
+  }
+  u[8] = h2f2<SX, SY>(ldlink(t16 + (size_t)f * V + site));
+}
+
+// 12-real 16-bit long link f at site, times (SX, SY), row 2 rebuilt with k
+template <int SX, int SY>
+__device__ __forceinline__ void load_long12_x2(const LoLinks &L, int f, size_t site, size_t V, float k,
+                                               float2 u[9]) {
+  const uint4 q = ldlink(L.f16_long + (size_t)f * V + site);
+  const uint2 t = ldlink(L.f16_long_tail2 + (size_t)f * V + site);
+  u[0] = h2f2<SX, SY>(q.x);
+  u[1] = h2f2<SX, SY>(q.y);
+  u[2] = h2f2<SX, SY>(q.z);
+  u[3] = h2f2<SX, SY>(q.w);
+  u[4] = h2f2<SX, SY>(t.x);
+  u[5] = h2f2<SX, SY>(t.y);
+  recon_row2(u, k);
+}
+
+// colour vector at i as broadcast pairs br[c] = s Re v_c (both lanes),
+// bi[c] = s Im v_c
+template <int VP>
+__device__ __forceinline__ void load_vec_bc(const void *base, int stride, int i, float s, float2 br[3],
+                                            float2 bi[3]) {
+  if (VP == kF32) {
+    const float2 *p = (const float2 *)base;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float2 v = ldg(p + (size_t)c * stride + i);
+      br[c] = make_float2(s * v.x, s * v.x);
+      bi[c] = make_float2(s * v.y, s * v.y);
+    }
+  } else {
+    const uint4 q = ldg((const uint4 *)base + i);
+    const float n = __uint_as_float(q.w) * (1.f / kI16) * s;
+    const unsigned w[3] = {q.x, q.y, q.z};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float2 r = h2f2<1, 1>(w[c]);
+      br[c] = __fmul2_rn(make_float2(r.x, r.x), make_float2(n, n));
+      bi[c] = __fmul2_rn(make_float2(r.y, r.y), make_float2(n, n));
+    }
+  }
+}
+
 // bytes of one site of a colour vector in each format
 constexpr int vec_bytes(int prec) { return prec == kF32 ? 24 : 16; }
 

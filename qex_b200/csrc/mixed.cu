@@ -417,6 +417,114 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
   }
 }
 
+// The 16-bit half sweep in packed FP32x2 arithmetic.  Per site and hop:
+//   forward  t_i = sum_j U_ij(x) v_j,             v = xin(x + d)
+//   backward q_i = sum_j conj(U_ji(x - d)) w_j,   w = xin(x - d)
+// accumulated as d = sum (t - q) = T + i S with T = sum (u Re v), S =
+// sum (u Im v) over (re, im) pairs u of the links: the backward link is
+// decoded directly as -conj(U) (its row 2 rebuilt with -k) so that its
+// terms add.  The long hops' vectors are scaled by long_scale / fat_scale,
+// so one set of accumulators carries both lists in fat units.
+template <int VP, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
+__global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo A) {
+  pdl_wait();
+  if (A.halt != nullptr && mx_halt(A.halt)) return;
+  const Geom &g = A.g;
+  const int nh = g.nh;
+  const size_t V = (size_t)g.V;
+  const size_t in_base = (size_t)(1 - A.po) * nh;
+  const size_t out_base = (size_t)A.po * nh;
+  const float rho = A.L.long_scale / A.L.fat_scale;
+  double dot = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+    int x[4], lex;
+    site_coords(g, A.po, k, x, lex);
+    float2 T[3], S[3], xsv[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      T[c] = make_float2(0.f, 0.f);
+      S[c] = make_float2(0.f, 0.f);
+    }
+    if (INIT) load_vec_cg<VP>(A.xs, A.sstride, k, xsv);
+#pragma unroll
+    for (int l = 0; l < NL; l++) {
+      const int mu = Hop<NL>::mu(l), len = Hop<NL>::len(l);
+      const bool is_long = (NL == 8) && (l & 1);
+      const int f = (NL == 8) ? (l >> 1) : l;
+      const int jf = nbr_half(g, x, lex, mu, len);
+      const int jb = nbr_half(g, x, lex, mu, -len);
+      const float s = is_long ? rho : 1.f;
+      float2 br[3], bi[3], u[9];
+      // forward hop
+      load_vec_bc<VP>(A.xin, A.istride, jf, s, br, bi);
+      if (is_long) {
+        if (R12)
+          load_long12_x2<1, 1>(A.L, f, out_base + k, V, long_sign_fwd(g, x, mu) * A.L.long_rc, u);
+        else
+          load_link18_x2<1, 1>(A.L.f16_long, A.L.f16_long_tail, f, out_base + k, V, u);
+      } else {
+        load_link18_x2<1, 1>(A.L.f16_fat, A.L.f16_fat_tail, f, out_base + k, V, u);
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          T[i] = __ffma2_rn(u[3 * i + j], br[j], T[i]);
+          S[i] = __ffma2_rn(u[3 * i + j], bi[j], S[i]);
+        }
+      }
+      // backward hop, link decoded as -conj(U)
+      load_vec_bc<VP>(A.xin, A.istride, jb, s, br, bi);
+      if (is_long) {
+        if (R12)
+          load_long12_x2<-1, 1>(A.L, f, in_base + jb, V, -long_sign_bck(g, x, mu) * A.L.long_rc, u);
+        else
+          load_link18_x2<-1, 1>(A.L.f16_long, A.L.f16_long_tail, f, in_base + jb, V, u);
+      } else {
+        load_link18_x2<-1, 1>(A.L.f16_fat, A.L.f16_fat_tail, f, in_base + jb, V, u);
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          T[i] = __ffma2_rn(u[3 * j + i], br[j], T[i]);
+          S[i] = __ffma2_rn(u[3 * j + i], bi[j], S[i]);
+        }
+      }
+    }
+    float2 o[3];
+    const float sf = HOP > 0 ? A.L.fat_scale : -A.L.fat_scale;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float2 d = make_float2(T[c].x - S[c].y, T[c].y + S[c].x);
+      float2 acc = INIT ? make_float2(A.b * xsv[c].x, A.b * xsv[c].y) : make_float2(0.f, 0.f);
+      acc.x = fmaf(sf, d.x, acc.x);
+      acc.y = fmaf(sf, d.y, acc.y);
+      o[c] = acc;
+    }
+    store_vec<OUTP>(A.out, A.ostride, k, o);
+    if (RED) {
+      float dd = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; c++) dd += xsv[c].x * o[c].x + xsv[c].y * o[c].y;
+      dot += (double)dd;
+    }
+  }
+  if (RED) {
+    double v[1] = {dot}, sm[1];
+    if (grid_reduce<1>(v, A.partials, A.ticket, sm) && threadIdx.x == 0) {
+      if (RED == 1) {
+        MxState *st = A.state;
+        st->pAp = sm[0];
+        st->alpha = st->r2 / sm[0];
+        st->itn += 1;
+      } else {
+        *A.dot_out = sm[0];
+      }
+    }
+  }
+}
+
 // Grid of a sloppy half sweep.  The 16-bit kernel runs exactly two waves of
 // resident blocks (occupancy from the runtime, so that no partial wave idles
 // SMs: on 32^4 two waves gave 5208 GB/s, 1.5 waves 4437); the FP32 kernel is
@@ -426,9 +534,14 @@ static int lo_grid(int nh) {
   static int resident = 0;  // one per kernel instantiation
   if (resident == 0) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, R12>,
-                                                      kBlock, 0) != cudaSuccess ||
-        n < 1) {
+    cudaError_t e;
+    if constexpr (PREC == kF16)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, R12>,
+                                                        kBlock, 0);
+    else
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, R12>,
+                                                        kBlock, 0);
+    if (e != cudaSuccess || n < 1) {
       cudaGetLastError();
       n = 4;
     }
@@ -443,12 +556,20 @@ static int lo_grid(int nh) {
 
 template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP>
 static void launch_lo(const DslashArgsLo &A, int) {
-  if (NL == 8 && A.L.recon12)
+  if constexpr (PREC == kF16) {
+    if (NL == 8 && A.L.recon12)
+      launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 1>,
+                 lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, A);
+    else
+      launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 0>,
+                 lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, A);
+  } else if (NL == 8 && A.L.recon12) {
     launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>,
                lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, A);
-  else
+  } else {
     launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>,
                lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, A);
+  }
   note_launch();
 }
 
