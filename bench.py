@@ -270,11 +270,15 @@ def run_ours(args, dims):
                                    "GFLOPs": round(v["GFLOPs"], 1), "us": round(v["seconds"] * 1e6, 1)}
                                for n, v in kt.items()}}
 
-    # e2e: the same solve through the C ABI with host buffers
-    bh = np.ascontiguousarray(b)
-    yh = np.zeros_like(bh)
+    # e2e: the same solve through the C ABI with host buffers in pinned
+    # memory: per solve the library copies the source's even half in and
+    # the whole solution field out
+    bh_t = torch.from_numpy(np.ascontiguousarray(b)).pin_memory()
+    yh_t = torch.zeros(b.shape, dtype=torch.complex128).pin_memory()
+    bh, yh = bh_t.numpy(), yh_t.numpy()
     kw = configs[[c[0] for c in configs].index(best)][1]
     e2e_times = []
+    s.solveEE(yh, bh, MASS, S.SolverParams(r2req=R2REQ, **kw))  # warm-up (staging buffers)
     for i in range(max(1, args.steps)):
         sp = S.SolverParams(r2req=R2REQ, **kw)
         torch.cuda.synchronize()
@@ -303,8 +307,8 @@ def run_ours(args, dims):
                 "fp64_time_s": results["fp64"]["time_s"],
                 "speedup_vs_fp64": results["fp64"]["time_s"] / value,
                 "roofline": roof, "cpu_baseline": cpu,
-                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(bh.nbytes),
-                        "d2h_bytes_per_step": int(yh.nbytes)},
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(bh.nbytes) // 2,
+                        "d2h_bytes_per_step": int(yh.nbytes), "host_memory": "pinned"},
                 "clocks": results[best]["clocks"],
                 "gpu_launches": int(results[best]["launches"])}
         print(json.dumps(line), flush=True)

@@ -95,6 +95,30 @@ static int stage_in(qexstag_links_s *g, int slot, const double *ptr, int mem,
   return QEXSTAG_OK;
 }
 
+// parity block par of a host field (QEX V=1 order: the nh sites of parity 0
+// first) into block par of a SoA slot; the slot's other block is not
+// written (the caller reads block par only)
+static int stage_in_block(qexstag_links_s *g, int slot, const double *ptr, int mem, int par,
+                          const double2 **dev) {
+  const Geom &geo = g->l->g;
+  if (mem == QEXSTAG_MEM_DEVICE) {
+    *dev = (const double2 *)ptr;
+    return QEXSTAG_OK;
+  }
+  void *soa, *aos;
+  const size_t bytes = sizeof(double2) * 3 * (size_t)geo.V;
+  const size_t half = sizeof(double2) * 3 * (size_t)geo.nh;
+  int rc;
+  if ((rc = g->ws.get(slot, bytes, &soa)) || (rc = g->ws.get(kSlotAos, bytes, &aos))) return rc;
+  QS_CUDA(cudaMemcpyAsync((char *)aos + par * half, (const char *)ptr + par * half, half, cudaMemcpyHostToDevice,
+                          stream()));
+  if ((rc = aos_to_soa((const double *)aos + (size_t)par * 6 * geo.nh, (double2 *)soa + (size_t)par * geo.nh,
+                       geo.nh, geo.V, 3)))
+    return rc;
+  *dev = (const double2 *)soa;
+  return QEXSTAG_OK;
+}
+
 static int stage_out_buf(qexstag_links_s *g, int slot, double *ptr, int mem, double2 **dev) {
   const Geom &geo = g->l->g;
   if (mem == QEXSTAG_MEM_DEVICE) {
@@ -462,7 +486,8 @@ static int solveXX_api(qexstag_links *g, int par, double *r, const double *x, do
   const double2 *dx;
   double2 *dr;
   Timer tm;
-  if ((rc = stage_in(g, kSlotIn0, x, mem, &dx))) return rc;
+  // solveXX reads x on parity par only
+  if ((rc = stage_in_block(g, kSlotIn0, x, mem, par, &dx))) return rc;
   if ((rc = stage_out_buf(g, kSlotOut0, r, mem, &dr))) return rc;
   int status = solve_xx(g, par, dr, dx, m, p, &st);
   if (status < 0) return status;
