@@ -402,7 +402,12 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
       dot += (double)d;
     }
   }
-  if (RED) {
+  if (RED == 3) {
+    __shared__ double sh3[32];
+    double v[1] = {dot};
+    block_sum<1>(v, sh3);
+    if (threadIdx.x == 0) A.partials[blockIdx.x] = v[0];
+  } else if (RED) {
     double v[1] = {dot}, s[1];
     if (grid_reduce<1>(v, A.partials, A.ticket, s) && threadIdx.x == 0) {
       if (RED == 1) {
@@ -510,7 +515,13 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
       dot += (double)dd;
     }
   }
-  if (RED) {
+  if (RED == 3) {
+    // per-block partial of Re <xs, out>, added up by the next kernel
+    __shared__ double sh3[32];
+    double v[1] = {dot};
+    block_sum<1>(v, sh3);
+    if (threadIdx.x == 0) A.partials[blockIdx.x] = v[0];
+  } else if (RED) {
     double v[1] = {dot}, sm[1];
     if (grid_reduce<1>(v, A.partials, A.ticket, sm) && threadIdx.x == 0) {
       if (RED == 1) {
@@ -554,40 +565,49 @@ static int lo_grid(int nh) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// returns the grid launched
 template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP>
-static void launch_lo(const DslashArgsLo &A, int) {
+static int launch_lo(const DslashArgsLo &A, int) {
+  int grid;
   if constexpr (PREC == kF16) {
-    if (NL == 8 && A.L.recon12)
-      launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 1>,
-                 lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, A);
-    else
-      launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 0>,
-                 lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, A);
+    if (NL == 8 && A.L.recon12) {
+      grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh);
+      launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 1>, grid, kBlock, A);
+    } else {
+      grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh);
+      launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 0>, grid, kBlock, A);
+    }
   } else if (NL == 8 && A.L.recon12) {
-    launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>,
-               lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh), kBlock, A);
+    grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh);
+    launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>, grid, kBlock, A);
   } else {
-    launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>,
-               lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh), kBlock, A);
+    grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh);
+    launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>, grid, kBlock, A);
   }
   note_launch();
+  return grid;
 }
 
 // the two half sweeps of the sloppy Schur operator:
 //   which 0: t = (2D)_{q,par} p                (out: PREC, hop +1)
 //   which 1: ap = 4 m2 p - (2D)_{par,q} t      (out: FP32, hop -1, pAp)
+//   red 3: per-block partials of <p, Ap> in partials[0 .. *blocks)
 template <int PREC, int NL>
-static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red) {
+static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int *blocks) {
   constexpr int VP = VecPrec<PREC>::v;
+  int used;
   if (which == 0) {
-    launch_lo<PREC, VP, NL, 1, 0, 0, VP>(A, grid);
+    used = launch_lo<PREC, VP, NL, 1, 0, 0, VP>(A, grid);
   } else if (red == 1) {
-    launch_lo<PREC, VP, NL, -1, 1, 1, kF32>(A, grid);
+    used = launch_lo<PREC, VP, NL, -1, 1, 1, kF32>(A, grid);
   } else if (red == 2) {
-    launch_lo<PREC, VP, NL, -1, 1, 2, kF32>(A, grid);
+    used = launch_lo<PREC, VP, NL, -1, 1, 2, kF32>(A, grid);
+  } else if (red == 3) {
+    used = launch_lo<PREC, VP, NL, -1, 1, 3, kF32>(A, grid);
   } else {
-    launch_lo<PREC, VP, NL, -1, 1, 0, kF32>(A, grid);
+    used = launch_lo<PREC, VP, NL, -1, 1, 0, kF32>(A, grid);
   }
+  if (blocks) *blocks = used;
   QS_LAUNCH_CHECK();
   return QEXSTAG_OK;
 }
@@ -595,7 +615,7 @@ static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red) {
 // sloppy Schur: ap (FP32 [3][nh]) = 4 m2 p - (2D)(2D) p on parity par,
 // p and t in format prec.
 int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void *p, void *t,
-             double m2, int red, MxState *state, const MxState *halt, double *dot_out) {
+             double m2, int red, MxState *state, const MxState *halt, double *dot_out, int *red_blocks) {
   const Geom &geo = g->l->g;
   DslashArgsLo A;
   A.g = geo;
@@ -617,9 +637,9 @@ int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void
   A.b = 0.f;
   int rc;
   if (prec == kF32)
-    rc = g->nl == 8 ? sloppy_half<kF32, 8>(0, A, grid, 0) : sloppy_half<kF32, 4>(0, A, grid, 0);
+    rc = g->nl == 8 ? sloppy_half<kF32, 8>(0, A, grid, 0, nullptr) : sloppy_half<kF32, 4>(0, A, grid, 0, nullptr);
   else
-    rc = g->nl == 8 ? sloppy_half<kF16, 8>(0, A, grid, 0) : sloppy_half<kF16, 4>(0, A, grid, 0);
+    rc = g->nl == 8 ? sloppy_half<kF16, 8>(0, A, grid, 0, nullptr) : sloppy_half<kF16, 4>(0, A, grid, 0, nullptr);
   if (rc) return rc;
   // half sweep 2
   A.po = par;
@@ -629,9 +649,11 @@ int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void
   A.out = ap;
   A.b = (float)(4.0 * m2);
   if (prec == kF32)
-    rc = g->nl == 8 ? sloppy_half<kF32, 8>(1, A, grid, red) : sloppy_half<kF32, 4>(1, A, grid, red);
+    rc = g->nl == 8 ? sloppy_half<kF32, 8>(1, A, grid, red, red_blocks)
+                    : sloppy_half<kF32, 4>(1, A, grid, red, red_blocks);
   else
-    rc = g->nl == 8 ? sloppy_half<kF16, 8>(1, A, grid, red) : sloppy_half<kF16, 4>(1, A, grid, red);
+    rc = g->nl == 8 ? sloppy_half<kF16, 8>(1, A, grid, red, red_blocks)
+                    : sloppy_half<kF16, 4>(1, A, grid, red, red_blocks);
   return rc;
 }
 
@@ -676,14 +698,40 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// rs -= alpha ap; xs += alpha p; then the reliable-update decision
+// alpha = r2 / pAp from the np per-block partials of <p, Ap> the half sweep
+// left (cg.nim:213-215): every block adds them in the same order, so all
+// get the same alpha; block 0 records pAp, alpha and the iteration
+__device__ __forceinline__ float mx_alpha(const double *pap, int np, MxState *st) {
+  __shared__ double sh_alpha;
+  if (threadIdx.x < 32) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += 32) s += __ldcg(pap + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) {
+      const double alpha = st->r2 / s;
+      sh_alpha = alpha;
+      if (blockIdx.x == 0) {
+        st->pAp = s;
+        st->alpha = alpha;
+        st->itn += 1;
+        st->r2old = st->r2;  // beta's denominator for mx_p_kernel
+      }
+    }
+  }
+  __syncthreads();
+  return (float)sh_alpha;
+}
+
+// rs -= alpha ap; xs += alpha p, with alpha from the half sweep's <p, Ap>
+// partials at pap (mx_alpha); |r|^2 per block into r2p[blockIdx.x]
 template <int PREC>
 __global__ void __launch_bounds__(kBlock)
     mx_update_kernel(float2 *__restrict__ rs, float2 *__restrict__ xs, const float2 *__restrict__ ap,
-                     const void *p, int n, MxState *st, double *partials, unsigned *ticket) {
+                     const void *p, int n, MxState *st, const double *pap, int np, double *r2p) {
   pdl_wait();
   if (mx_halt(st)) return;
-  const float alpha = (float)st->alpha;
+  const float alpha = mx_alpha(pap, np, st);
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float2 pv[3];
@@ -703,35 +751,65 @@ __global__ void __launch_bounds__(kBlock)
     }
     s += (double)acc;
   }
-  double v[1] = {s}, o[1];
-  if (grid_reduce<1>(v, partials, ticket, o) && threadIdx.x == 0) {
-    const double r2 = o[0];
-    st->r2old = st->r2;
-    st->r2 = r2;
-    if (!isfinite(r2)) {
-      st->nan = 1;
-      st->done = 1;
-      return;
-    }
-    const double rn = sqrt(r2);
-    st->rNorm = rn;
-    st->maxrr = fmax(st->maxrr, rn);
-    st->maxrx = fmax(st->maxrx, rn);
-    const bool ux = rn < st->delta * st->r0Norm && st->r0Norm <= st->maxrx;
-    const bool ur = (rn < st->delta * st->maxrr && st->r0Norm <= st->maxrr) || ux;
-    if (ur || r2 <= st->r2stop || st->itn >= st->maxits) {
-      st->pending = 1;
-    } else {
-      st->beta = r2 / st->r2old;
-    }
-  }
+  __shared__ double sh[32];
+  double v[1] = {s};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) r2p[blockIdx.x] = v[0];
 }
 
+// |r|^2 from the update's np per-block partials at r2p (added in the same
+// order by every block), the reliable-update test (|r| against delta times
+// the largest |r| since the last update), then p = r + beta p unless an
+// update is due.  Block 0 records the state.  The fields other blocks read are not written
+// here (r0Norm, delta, r2stop, itn, r2old) or are maxima that come out the
+// same whether read before or after block 0's write (maxrr, maxrx).
 template <int PREC>
-__global__ void mx_p_kernel(const float2 *__restrict__ rs, void *p, int n, const MxState *st) {
+__global__ void mx_p_kernel(const float2 *__restrict__ rs, void *p, int n, MxState *st, const double *r2p,
+                            int np) {
   pdl_wait();
   if (mx_halt(st)) return;
-  const float beta = (float)st->beta;
+  __shared__ float sh_beta;
+  __shared__ int sh_go;
+  if (threadIdx.x < 32) {
+    double r2 = 0.0;
+    for (int i = threadIdx.x; i < np; i += 32) r2 += __ldcg(r2p + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+    if (threadIdx.x == 0) {
+      int go = 0;
+      double beta = 0.0;
+      if (!isfinite(r2)) {
+        if (blockIdx.x == 0) {
+          st->r2 = r2;
+          st->nan = 1;
+          st->done = 1;
+        }
+      } else {
+        const double rn = sqrt(r2);
+        const double maxrr = fmax(st->maxrr, rn), maxrx = fmax(st->maxrx, rn);
+        const bool ux = rn < st->delta * st->r0Norm && st->r0Norm <= maxrx;
+        const bool ur = (rn < st->delta * maxrr && st->r0Norm <= maxrr) || ux;
+        const bool pend = ur || r2 <= st->r2stop || st->itn >= st->maxits;
+        beta = r2 / st->r2old;
+        go = pend ? 0 : 1;
+        if (blockIdx.x == 0) {
+          st->r2 = r2;
+          st->rNorm = rn;
+          st->maxrr = maxrr;
+          st->maxrx = maxrx;
+          if (pend)
+            st->pending = 1;
+          else
+            st->beta = beta;
+        }
+      }
+      sh_beta = (float)beta;
+      sh_go = go;
+    }
+  }
+  __syncthreads();
+  if (!sh_go) return;
+  const float beta = sh_beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float2 pv[3];
     load_vec_cg<PREC>(p, n, i, pv);
@@ -887,10 +965,15 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   const int every = check_interval(nh);
   for (;;) {
     for (int i = 0; i < every; i++) {
-      if ((rc = schur_lo(g, PREC, par, ap, pp, pt, m2, 1, st, st, nullptr))) return rc;
+      int np = 0;
+      if ((rc = schur_lo(g, PREC, par, ap, pp, pt, m2, 3, st, st, nullptr, &np))) return rc;
+      // <p, Ap> partials in the first kMaxRedBlocks doubles of the scratch,
+      // the update's |r|^2 partials after them; each summed by the next kernel
+      double *r2p = red_partials() + kMaxRedBlocks;
       launch_pdl(mx_update_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)pp, nh, st,
-                 red_partials(), red_tickets());
-      launch_pdl(mx_p_kernel<VP>, egrid, kBlock, (const float2 *)rs, (void *)pp, nh, (const MxState *)st);
+                 (const double *)red_partials(), np, r2p);
+      launch_pdl(mx_p_kernel<VP>, egrid, kBlock, (const float2 *)rs, (void *)pp, nh, st, (const double *)r2p,
+                 grid);
       note_launch(2);
     }
     QS_LAUNCH_CHECK();
@@ -994,7 +1077,8 @@ int bench_schur(qexstag_links_s *g, int prec, int nrep, double m2, double *sec) 
   auto once = [&]() -> int {
     if (prec == 0)
       return schur64(g, 0, VecD{(double2 *)pc, nh}, CVecD{(const double2 *)pa, nh}, VecD{(double2 *)pb, nh}, m2);
-    return schur_lo(g, prec == 1 ? kF32 : kF16, 0, (float2 *)pc, pa, pb, m2, 0, nullptr, nullptr, nullptr);
+    return schur_lo(g, prec == 1 ? kF32 : kF16, 0, (float2 *)pc, pa, pb, m2, 0, nullptr, nullptr, nullptr,
+                    nullptr);
   };
   for (int i = 0; i < 2; i++)
     if ((rc = once())) return rc;
