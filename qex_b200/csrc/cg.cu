@@ -105,20 +105,28 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// read the device CgState back to the host (pinned staging)
-int read_state(const CgState *dst, CgState *host) {
-  double *h = host_results();
-  static_assert(sizeof(CgState) <= sizeof(double) * kNumResults, "state too large");
-  QS_CUDA(cudaMemcpyAsync(h, dst, sizeof(CgState), cudaMemcpyDeviceToHost, stream()));
-  QS_CUDA(cudaStreamSynchronize(stream()));
-  std::memcpy(host, h, sizeof(CgState));
-  return QEXSTAG_OK;
-}
+static_assert(sizeof(CgState) <= sizeof(double) * kNumResults, "state too large for the staging buffer");
 
 int write_state(CgState *dst, const CgState &host) {
   double *h = host_results();
   std::memcpy(h, &host, sizeof(CgState));
   QS_CUDA(cudaMemcpyAsync(dst, h, sizeof(CgState), cudaMemcpyHostToDevice, stream()));
+  return QEXSTAG_OK;
+}
+
+StateSnapshot::~StateSnapshot() {
+  if (ev) cudaEventDestroy(ev);
+}
+int StateSnapshot::start(const void *dev, size_t bytes) {
+  if (bytes > sizeof(double) * kNumResults) return fail(QEXSTAG_ERR_ARG, "state snapshot too large");
+  if (!ev) QS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  QS_CUDA(cudaMemcpyAsync(host_results(), dev, bytes, cudaMemcpyDeviceToHost, stream()));
+  QS_CUDA(cudaEventRecord(ev, stream()));
+  return QEXSTAG_OK;
+}
+int StateSnapshot::wait(void *host, size_t bytes) {
+  QS_CUDA(cudaEventSynchronize(ev));
+  std::memcpy(host, host_results(), bytes);
   return QEXSTAG_OK;
 }
 
@@ -156,18 +164,28 @@ int cg64(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, 
   QS_LAUNCH_CHECK();
   const int every = check_interval(nh);
   const int pgrid = grid_for(nh, kBlock, 8);
-  for (;;) {
+  auto batch = [&]() -> int {
     for (int i = 0; i < every; i++) {
       launch_pdl(cg_p_kernel, pgrid, kBlock, (const double2 *)r.p, r.stride, p.p, p.stride, nh,
                  (const CgState *)st);
       note_launch();
-      if ((rc = schur64(g, par, ap, cv(p), t, m2, kRedCgPAp, st, &st->done))) return rc;
+      int rc2 = schur64(g, par, ap, cv(p), t, m2, kRedCgPAp, st, &st->done);
+      if (rc2) return rc2;
       launch_pdl(cg_xr_kernel, grid, kBlock, x.p, x.stride, r.p, r.stride, (const double2 *)p.p, p.stride,
                  (const double2 *)ap.p, ap.stride, nh, st, red_partials(), red_tickets());
       note_launch();
     }
     QS_LAUNCH_CHECK();
-    if ((rc = read_state(st, &hs))) return rc;
+    return QEXSTAG_OK;
+  };
+  // The state is read one batch behind: the next batch is queued before
+  // the host waits for the snapshot, so the GPU does not idle during the
+  // check; once the solve is done that batch's kernels return at once.
+  StateSnapshot snap;
+  if ((rc = batch())) return rc;
+  for (;;) {
+    if ((rc = snap.start(st, sizeof(CgState))) || (rc = batch()) || (rc = snap.wait(&hs, sizeof(CgState))))
+      return rc;
     if (hs.done) break;
   }
   out->iterations = hs.itn;

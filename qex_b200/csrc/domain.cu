@@ -122,7 +122,6 @@ constexpr int kValOff = kMaxSet;
 constexpr int kStateOff = kMaxSet + 8;
 constexpr size_t kDevScalarBytes = sizeof(double) * kStateOff + sizeof(CgState);
 
-int read_state(const CgState *dst, CgState *host);
 int write_state(CgState *dst, const CgState &host);
 int check_interval(int nh);
 
@@ -744,10 +743,19 @@ int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x,
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, stream());
-  while (!hs.done) {
-    for (int i = 0; i < every && !rc; i++) rc = cg_iteration(doms, n, xv.data(), rv.data(), pv.data(), ap.data(),
-                                                            tv.data(), m2, st);
-    if (rc || (rc = read_state(st, &hs))) break;
+  auto batch = [&]() -> int {
+    int rc2 = QEXSTAG_OK;
+    for (int i = 0; i < every && !rc2; i++)
+      rc2 = cg_iteration(doms, n, xv.data(), rv.data(), pv.data(), ap.data(), tv.data(), m2, st);
+    return rc2;
+  };
+  // the state is read one batch behind (the next batch is queued first);
+  // every rank reads the same all-reduced state, so all queue the same
+  // batches, and those past convergence return at once
+  StateSnapshot snap;
+  if (!hs.done) rc = batch();
+  while (!rc && !hs.done) {
+    if ((rc = snap.start(st, sizeof(CgState))) || (rc = batch()) || (rc = snap.wait(&hs, sizeof(CgState)))) break;
   }
   cudaEventRecord(e1, stream());
   cudaEventSynchronize(e1);

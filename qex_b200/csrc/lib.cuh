@@ -102,6 +102,18 @@ int vredot(CVecD x, CVecD y, int n, double *host);
 int vdiffnorm2(CVecD a, CVecD b, int n, double *host);
 
 // ---- solvers (cg.cu) ----
+// Asynchronous read of a solver's device state: start() queues a copy into
+// the pinned staging buffer and records an event; wait() blocks on that
+// event only, so work queued after start() keeps the GPU busy meanwhile.
+struct StateSnapshot {
+  cudaEvent_t ev = nullptr;
+  StateSnapshot() = default;
+  StateSnapshot(const StateSnapshot &) = delete;
+  StateSnapshot &operator=(const StateSnapshot &) = delete;
+  ~StateSnapshot();
+  int start(const void *dev, size_t bytes);
+  int wait(void *host, size_t bytes);
+};
 struct CgOut {
   int iterations;
   double r2;  // recursive |r|^2/|b|^2 at exit

@@ -915,14 +915,7 @@ __global__ void mx_p_reliable_kernel(const float2 *__restrict__ rs, void *p, int
 
 __global__ void mx_clear_pending_kernel(MxState *st) { st->pending = 0; }
 
-int read_mx(const MxState *d, MxState *h) {
-  double *buf = host_results();
-  static_assert(sizeof(MxState) <= sizeof(double) * kNumResults, "state too large");
-  QS_CUDA(cudaMemcpyAsync(buf, d, sizeof(MxState), cudaMemcpyDeviceToHost, stream()));
-  QS_CUDA(cudaStreamSynchronize(stream()));
-  std::memcpy(h, buf, sizeof(MxState));
-  return QEXSTAG_OK;
-}
+static_assert(sizeof(MxState) <= sizeof(double) * kNumResults, "state too large for the staging buffer");
 
 int check_interval(int nh);
 
@@ -963,10 +956,11 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   note_launch();
   QS_LAUNCH_CHECK();
   const int every = check_interval(nh);
-  for (;;) {
+  auto batch = [&]() -> int {
     for (int i = 0; i < every; i++) {
       int np = 0;
-      if ((rc = schur_lo(g, PREC, par, ap, pp, pt, m2, 3, st, st, nullptr, &np))) return rc;
+      int rc2 = schur_lo(g, PREC, par, ap, pp, pt, m2, 3, st, st, nullptr, &np);
+      if (rc2) return rc2;
       // <p, Ap> partials in the first kMaxRedBlocks doubles of the scratch,
       // the update's |r|^2 partials after them; each summed by the next kernel
       double *r2p = red_partials() + kMaxRedBlocks;
@@ -977,7 +971,17 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
       note_launch(2);
     }
     QS_LAUNCH_CHECK();
-    if ((rc = read_mx(st, &hs))) return rc;
+    return QEXSTAG_OK;
+  };
+  // The state is read one batch behind: the next batch is queued before the
+  // host waits for the snapshot.  When the snapshot shows the solve done or
+  // a reliable update due, that batch's kernels have returned at once
+  // (done / pending), and the update is queued after them.
+  StateSnapshot snap;
+  if ((rc = batch())) return rc;
+  for (;;) {
+    if ((rc = snap.start(st, sizeof(MxState))) || (rc = batch()) || (rc = snap.wait(&hs, sizeof(MxState))))
+      return rc;
     if (hs.done) break;
     if (!hs.pending) continue;
     // reliable update: fold the increment in, FP64 true residual
@@ -991,8 +995,7 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
     mx_clear_pending_kernel<<<1, 1, 0, stream()>>>(st);
     note_launch(4);
     QS_LAUNCH_CHECK();
-    if ((rc = read_mx(st, &hs))) return rc;
-    if (hs.done) break;
+    if ((rc = batch())) return rc;
   }
   out->iterations = hs.itn;
   out->r2 = hs.b2 > 0 ? hs.r2 / hs.b2 : 0.0;
