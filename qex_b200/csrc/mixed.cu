@@ -274,17 +274,17 @@ __device__ __forceinline__ bool mx_halt(const MxState *st) { return st->done || 
 // are kept apart so that the FP16 list scales multiply them once per site.
 // ---------------------------------------------------------------------------
 
-// Resident blocks per SM asked of ptxas: the 16-bit kernel is instruction-
-// heavy for the bytes it moves and gains from occupancy (4 blocks: 64
-// registers, 4450 GB/s on 32^4 against 4090 GB/s with 72-80 registers, same
-// grid); the FP32 kernel runs at the copy bandwidth with its natural 72
-// registers.  (Splitting a site's forward and backward hops over two threads
-// was slower: 3640-3720 GB/s.)
+// dslash_lo_kernel serves the FP32 links (it runs at the copy bandwidth with
+// its natural registers); 16-bit links go to dslash_x2_kernel below.  The
+// 16-bit kernel is instruction-heavy for the bytes it moves and gains from
+// occupancy: 4 resident blocks of 64 registers (with scalar arithmetic this
+// gave 4450 GB/s on 32^4 against 4090 GB/s at 72-80 registers; splitting a
+// site's forward and backward hops over two threads gave 3640-3720 GB/s).
 
 // Format of the sloppy solver's vectors p and t for a link precision: the
-// same as the links, except that with 16-bit links the vectors may be kept
-// in FP32 (QS_HALF_VEC_BITS = 32), trading a few percent of traffic for the
-// iterations that 16-bit vectors cost.
+// same as the links.  With 16-bit links the vectors can be built in FP32
+// (QS_HALF_VEC_BITS = 32); on 32^4 that keeps the iteration count (2754)
+// and slows the Schur operator (90.1 against 86.2 us), so 16 is the default.
 #ifndef QS_HALF_VEC_BITS
 #define QS_HALF_VEC_BITS 16
 #endif
