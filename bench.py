@@ -267,7 +267,9 @@ def run_ours(args, dims):
             "bytes_per_even_site": k["bytes_per_even_site"],
             "seconds_per_call": k["seconds"],
             "all_precisions": {n: {"GBps": round(v["GBps"], 1), "frac": round(v["GBps"] / peak, 4),
-                                   "GFLOPs": round(v["GFLOPs"], 1), "us": round(v["seconds"] * 1e6, 1)}
+                                   "GFLOPs": round(v["GFLOPs"], 1), "us": round(v["seconds"] * 1e6, 1),
+                                   "GBps_no_reuse": round(v["GBps_no_reuse"], 1),
+                                   "no_reuse_bytes_per_even_site": v["no_reuse_bytes_per_even_site"]}
                                for n, v in kt.items()}}
 
     # e2e: the same solve through the C ABI with host buffers in pinned

@@ -22,6 +22,15 @@ BYTES = {  # (nlinks, prec) -> bytes per even site per Schur call
     (4, 0): 2544, (4, 1): 1272, (4, 2): 664,
 }
 NAMES = {0: "fp64", 1: "fp32", 2: "fp16"}
+VEC_BYTES = {0: 48, 1: 24, 2: 16}  # one site of the input vector per precision
+
+
+def no_reuse_bytes_per_site(nlinks: int, prec: int, recon12: bool = True) -> int:
+    """The same count with every neighbour's input vector charged (8 naive or
+    16 fat+Naik per output site and half sweep, no cache reuse), the figure
+    other staggered codes quote: FP64 fat+Naik 3120 B per half sweep."""
+    hops = 16 if nlinks == 8 else 8
+    return bytes_per_site(nlinks, prec, recon12) + 2 * (hops - 1) * VEC_BYTES[prec]
 
 
 def bytes_per_site(nlinks: int, prec: int, recon12: bool = True) -> int:
@@ -36,8 +45,10 @@ def time_schur(stag, nh: int, precs=(0, 1, 2), nrep: int = 20, m2: float = 1e-4)
     for p in precs:
         sec = stag.bench_schur(p, nrep, m2)
         bps = bytes_per_site(stag.nlinks, p, stag.recon12)
+        nrb = no_reuse_bytes_per_site(stag.nlinks, p, stag.recon12)
         out[NAMES[p]] = {"seconds": sec, "bytes_per_even_site": bps,
                          "GBps": bps * nh / sec / 1e9,
+                         "no_reuse_bytes_per_even_site": nrb, "GBps_no_reuse": nrb * nh / sec / 1e9,
                          "GFLOPs": (2 * (1146 if stag.nlinks == 8 else 570)) * nh / sec / 1e9}
     return out
 
