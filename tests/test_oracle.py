@@ -247,10 +247,27 @@ def _action(o, phi, m):
     return np.vdot(phi[: V // 2], y[: V // 2]).real
 
 
+def _su3_generators():
+    """The 8 anti-Hermitian traceless generators i lambda_a (Gell-Mann)."""
+    lam = np.zeros((8, 3, 3), dtype=np.complex128)
+    lam[0][0, 1] = lam[0][1, 0] = 1
+    lam[1][0, 1], lam[1][1, 0] = -1j, 1j
+    lam[2][0, 0], lam[2][1, 1] = 1, -1
+    lam[3][0, 2] = lam[3][2, 0] = 1
+    lam[4][0, 2], lam[4][2, 0] = -1j, 1j
+    lam[5][1, 2] = lam[5][2, 1] = 1
+    lam[6][1, 2], lam[6][2, 1] = -1j, 1j
+    lam[7] = np.diag([1, 1, -2]) / np.sqrt(3)
+    return 1j * lam
+
+
 @pytest.mark.parametrize("naik", [False, True])
 def test_force_finite_difference(naik):
-    """dS/deps for U_k(x) -> exp(eps T) U_k(x) equals ReTr[T f_k(x)^dagger]/8
-    with f the force fermForce returns (QEX's psi carries a factor 4)."""
+    """dS/deps for U_k(x) -> exp(eps T_a) U_k(x) equals ReTr[T_a f_k(x)^dagger]/8
+    with f the force fermForce returns (QEX's psi carries a factor 4): central
+    differences at eps = 1e-5 along all 8 su(3) generators on 64 seeded
+    (site, direction, link kind) entries (with Naik links, k runs over the
+    interleaved fat and long fields)."""
     dims = (4, 4, 4, 4)
     V = F.volume(dims)
     g = _links(dims, naik, seed=13)
@@ -261,16 +278,18 @@ def test_force_finite_difference(naik):
     f = np.zeros_like(g)
     o.force(f, phi, m, 1e-28)
     rng = np.random.default_rng(19)
+    entries = set()
+    while len(entries) < 64:
+        entries.add((int(rng.integers(0, g.shape[0])), int(rng.integers(0, V))))
+    gens = _su3_generators()
     eps = 1e-5
-    for trial in range(6):
-        k = int(rng.integers(0, g.shape[0]))
-        s = int(rng.integers(0, V))
-        T = F.rand_tah(1, rng)[0]
-        vals = []
-        for e in (eps, -eps):
-            gp = g.copy()
-            gp[k, s] = F.exp_ah(T[None], e)[0] @ g[k, s]
-            vals.append(_action(O.Oracle(dims, gp), phi, m))
-        fd = (vals[0] - vals[1]) / (2 * eps)
-        an = np.trace(T @ np.conj(f[k, s]).T).real / 8
-        assert abs(fd - an) <= 1e-7 * max(abs(an), 1e-3), (k, s, fd, an)
+    for k, s in sorted(entries):
+        for a, T in enumerate(gens):
+            vals = []
+            for e in (eps, -eps):
+                gp = g.copy()
+                gp[k, s] = F.exp_ah(T[None], e)[0] @ g[k, s]
+                vals.append(_action(O.Oracle(dims, gp), phi, m))
+            fd = (vals[0] - vals[1]) / (2 * eps)
+            an = np.trace(T @ np.conj(f[k, s]).T).real / 8
+            assert abs(fd - an) <= 1e-7 * max(abs(an), 1.0), (k, s, a, fd, an)
