@@ -444,6 +444,15 @@ int qexstag_kinetic_action(qexstag_layout *l, const double *p, int mem, double *
    the same calls in the same order. */
 typedef struct qexstag_domain_s qexstag_domain;
 int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nlinks, qexstag_domain **out);
+/* Split along t, then z (QEX's rankGeom over several directions): grid[0]
+   ranks along z and grid[1] along t, rank = rz + grid[0] rt holding z rows
+   [rz Z, (rz+1) Z) of slices [rt T, (rt+1) T), Z = L2/grid[0] and T as
+   above (both even, at least 6 with Naik links and 4 without); its local
+   lattice is {L0, L1, Z, T}.  Ghost rows in z are exchanged after the t
+   ghosts, so the corners come from the diagonal neighbours; grid[0] = 1
+   keeps z ghosts, exchanged with the rank itself. */
+int qexstag_domain_create_zt(const int global_dims[4], const int grid[2], int rank, int nlinks,
+                             qexstag_domain **out);
 int qexstag_domain_destroy(qexstag_domain *d);
 int qexstag_domain_local_dims(const qexstag_domain *d, int dims[4]);
 /* All nranks domains in this process (rank order), on the current device:

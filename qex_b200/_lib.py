@@ -147,6 +147,7 @@ SIGNATURES = {
     "qexstag_momenta_heatbath": (I, [P, P, C.c_ulonglong, C.c_ulonglong, I]),
     "qexstag_kinetic_action": (I, [P, P, I, DP]),
     "qexstag_domain_create": (I, [C.POINTER(C.c_int), I, I, I, C.POINTER(P)]),
+    "qexstag_domain_create_zt": (I, [C.POINTER(C.c_int), C.POINTER(C.c_int), I, I, C.POINTER(P)]),
     "qexstag_domain_destroy": (I, [P]),
     "qexstag_domain_local_dims": (I, [P, C.POINTER(C.c_int)]),
     "qexstag_domain_connect_local": (I, [PP, I]),

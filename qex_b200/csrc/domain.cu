@@ -29,7 +29,20 @@
 // CG): each domain's interior partial sum goes to a slot, one thread adds
 // the slots in rank order, NCCL all-reduces that value in place, and the
 // next kernel finishes alpha or beta, so an iteration makes no host round
-// trip and the host reads the state every few iterations.  NCCL is resolved at run time
+// trip and the host reads the state every few iterations.
+//
+// Along t, then z: qexstag_domain_create_zt splits the lattice over a grid
+// of Rz x Rt ranks (rank = rz + Rz rt), each holding Z = L2 / Rz by T =
+// L3 / Rt slabs extended by h ghost rows in z as well.  The exchange fills
+// the t ghost slices first (whole slices, z ghost rows included) and then
+// the z ghost rows of every slice (t ghost slices included), so the corner
+// regions receive the diagonal neighbour's sites by way of the z
+// neighbour's t ghosts.  Within a t slice each (z, t) row of L0 L1 / 2 sites
+// of a parity is contiguous, so a z face is a pitched 2D copy, packed into a
+// contiguous buffer for NCCL.  Both sweeps then run on the whole extended
+// slab after the exchange (no overlap); the values they produce on z ghost
+// rows are finite and never read, and every sum skips those rows.  A grid
+// with Rz = 1 still carries z ghosts and exchanges them with itself.  NCCL is resolved at run time
 // from the libnccl.so.2 already loaded in the process (the one torch
 // carries) or the system's, so the library does not link a second copy.
 #include <dlfcn.h>
@@ -97,9 +110,12 @@ static int nccl_fail(ncclResult_t r, const char *what) {
 struct qexstag_domain_s {
   int gdims[4];
   int nranks, rank, nl, h, T;
-  qexstag_layout_s *ext = nullptr;  // extended lattice (T + 2h slices)
+  int Rz = 1, Rt = 1, rz = 0, rt = 0;  // rank grid (z, t) and this rank's place
+  int Z = 0, hz = 0;                // interior z extent and z ghost depth (0: t only)
+  qexstag_layout_s *ext = nullptr;  // extended lattice (Z + 2hz rows, T + 2h slices)
   qexstag_links_s *g = nullptr;     // links on the extended lattice
-  qexstag_domain_s *up = nullptr, *down = nullptr;  // in-process neighbours
+  qexstag_domain_s *up = nullptr, *down = nullptr;    // in-process t neighbours
+  qexstag_domain_s *zup = nullptr, *zdown = nullptr;  // in-process z neighbours
   ncclComm_t comm = nullptr;        // inter-process neighbours
   bool connected = false;
   std::vector<qs::Geom> local;      // geometry of the T-slice local lattice
@@ -112,7 +128,8 @@ namespace qs {
 
 // workspace slots of a domain's link handle
 enum DomainSlot {
-  kDmIn = kSlotLast + 700, kDmOut, kDmT, kDmFull, kDmX, kDmR, kDmP, kDmAp, kDmSoa, kDmLinks
+  kDmIn = kSlotLast + 700, kDmOut, kDmT, kDmFull, kDmX, kDmR, kDmP, kDmAp, kDmSoa, kDmLinks,
+  kDmPack  // four NCCL z-face buffers (send down, send up, receive down, receive up)
 };
 
 // layout of a domain's device scalars (dsum): the partial sums of up to
@@ -125,12 +142,94 @@ constexpr size_t kDevScalarBytes = sizeof(double) * kStateOff + sizeof(CgState);
 int write_state(CgState *dst, const CgState &host);
 int check_interval(int nh);
 
-static size_t slice_half(const qexstag_domain_s *d) {
-  return (size_t)d->gdims[0] * d->gdims[1] * d->gdims[2] / 2;
+// sites of one parity in one (z, t) row, and in one t slice of the
+// extended lattice
+static size_t row_half(const qexstag_domain_s *d) { return (size_t)d->gdims[0] * d->gdims[1] / 2; }
+static size_t slice_half(const qexstag_domain_s *d) { return row_half(d) * (size_t)(d->Z + 2 * d->hz); }
+static int rank_of(const qexstag_domain_s *d, int rz, int rt) {
+  return (rz + d->Rz) % d->Rz + d->Rz * ((rt + d->Rt) % d->Rt);
+}
+
+// z faces: rows [row0, row0 + hz) of every t slice of parity block par, for
+// components c0 .. c0 + nc - 1, to or from a contiguous buffer
+// [nc][Te][hz * P]
+__global__ void face_copy_kernel(double2 *field, size_t V, size_t base, size_t pitch, double2 *buf, int nc,
+                                 int rows, size_t width, int to_buf) {
+  const size_t per = (size_t)rows * width, n = (size_t)nc * per;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = i / per, rem = i - c * per, s = rem / width, j = rem - s * width;
+    const size_t f = c * V + base + s * pitch + j;
+    if (to_buf)
+      buf[i] = field[f];
+    else
+      field[f] = buf[i];
+  }
+}
+
+static int find_in_set(qexstag_domain_s *const *ds, int n, const qexstag_domain_s *d) {
+  for (int j = 0; j < n; j++)
+    if (ds[j] == d) return j;
+  return -1;
+}
+
+// z ghost rows of every t slice of one parity block (after the t ghosts)
+static int exchange_z(qexstag_domain_s *const *ds, int n, double2 *const *base, int ncomp, int par,
+                      cudaStream_t s) {
+  const qexstag_domain_s *d0 = ds[0];
+  const size_t P = row_half(d0), pitch = slice_half(d0), width = (size_t)d0->hz * P;
+  const int rows = d0->T + 2 * d0->h, Z = d0->Z, hz = d0->hz;
+  for (int k = 0; k < n; k++) {
+    qexstag_domain_s *d = ds[k];
+    const size_t V = (size_t)d->ext->g.V, off = (size_t)par * d->ext->g.nh;
+    if (d->comm) {
+      const int upr = rank_of(d, d->rz + 1, d->rt), dnr = rank_of(d, d->rz - 1, d->rt);
+      for (int c0 = 0; c0 < ncomp; c0 += 3) {
+        const int nc = std::min(3, ncomp - c0);
+        const size_t face = (size_t)nc * rows * width;
+        void *pb;
+        int rc = d->g->ws.get(kDmPack, sizeof(double2) * 4 * (size_t)3 * rows * width, &pb);
+        if (rc) return rc;
+        double2 *sdn = (double2 *)pb, *sup = sdn + face, *rdn = sup + face, *rup = rdn + face;
+        double2 *f = base[k] + (size_t)c0 * V;
+        const int grid = grid_for((long)face);
+        // my lowest interior rows go down, my highest up
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off + (size_t)hz * P, pitch, sdn, nc, rows, width, 1);
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off + (size_t)Z * P, pitch, sup, nc, rows, width, 1);
+        note_launch(2);
+        QS_LAUNCH_CHECK();
+        QS_NCCL(nccl().groupStart());
+        QS_NCCL(nccl().send(sdn, 2 * face, ncclDouble, dnr, d->comm, s));
+        QS_NCCL(nccl().recv(rup, 2 * face, ncclDouble, upr, d->comm, s));
+        QS_NCCL(nccl().send(sup, 2 * face, ncclDouble, upr, d->comm, s));
+        QS_NCCL(nccl().recv(rdn, 2 * face, ncclDouble, dnr, d->comm, s));
+        QS_NCCL(nccl().groupEnd());
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off, pitch, rdn, nc, rows, width, 0);
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off + (size_t)(hz + Z) * P, pitch, rup, nc, rows, width, 0);
+        note_launch(2);
+        QS_LAUNCH_CHECK();
+      }
+    } else {
+      const int ku = find_in_set(ds, n, d->zup), kd = find_in_set(ds, n, d->zdown);
+      if (ku < 0 || kd < 0) return fail(QEXSTAG_ERR_STATE, "domain: a z neighbour is not in the call's domain set");
+      for (int c = 0; c < ncomp; c++) {
+        double2 *f = base[k] + (size_t)c * V + off;
+        const double2 *fd = base[kd] + (size_t)c * V + off;
+        const double2 *fu = base[ku] + (size_t)c * V + off;
+        // lower ghost rows <- the z-down neighbour's highest interior rows, upper <- z-up's lowest
+        QS_CUDA(cudaMemcpy2DAsync(f, pitch * sizeof(double2), fd + (size_t)Z * P, pitch * sizeof(double2),
+                                  width * sizeof(double2), rows, cudaMemcpyDeviceToDevice, s));
+        QS_CUDA(cudaMemcpy2DAsync(f + (size_t)(hz + Z) * P, pitch * sizeof(double2), fu + (size_t)hz * P,
+                                  pitch * sizeof(double2), width * sizeof(double2), rows, cudaMemcpyDeviceToDevice,
+                                  s));
+      }
+    }
+  }
+  return QEXSTAG_OK;
 }
 
 // one parity block's ghost exchange of ncomp component arrays, each with
-// stride V_ext, of the fields at base[k] of each domain of the set
+// stride V_ext, of the fields at base[k] of each domain of the set: t ghost
+// slices, then (domains split along z) the z ghost rows of every slice
 static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, int ncomp, int par,
                     cudaStream_t s) {
   const size_t sh = slice_half(ds[0]);
@@ -140,7 +239,7 @@ static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, in
     const size_t cnt = d->h * sh;  // sites per face per component
     if (d->comm) {
       QS_NCCL(nccl().groupStart());
-      const int upr = (d->rank + 1) % d->nranks, dnr = (d->rank + d->nranks - 1) % d->nranks;
+      const int upr = rank_of(d, d->rz, d->rt + 1), dnr = rank_of(d, d->rz, d->rt - 1);
       for (int c = 0; c < ncomp; c++) {
         double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
         // my top interior slices -> up's lower ghosts; my bottom -> down's upper
@@ -152,11 +251,7 @@ static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, in
       QS_NCCL(nccl().groupEnd());
     } else {
       // pull from the in-process neighbours
-      int ku = -1, kd = -1;
-      for (int j = 0; j < n; j++) {
-        if (ds[j] == d->up) ku = j;
-        if (ds[j] == d->down) kd = j;
-      }
+      const int ku = find_in_set(ds, n, d->up), kd = find_in_set(ds, n, d->down);
       if (ku < 0 || kd < 0) return fail(QEXSTAG_ERR_STATE, "domain: a neighbour is not in the call's domain set");
       for (int c = 0; c < ncomp; c++) {
         double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
@@ -168,6 +263,7 @@ static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, in
       }
     }
   }
+  if (ds[0]->hz > 0) return exchange_z(ds, n, base, ncomp, par, s);
   return QEXSTAG_OK;
 }
 
@@ -186,15 +282,15 @@ static int allreduce_sum(qexstag_domain_s *const *ds, int n, const double *vals,
   return QEXSTAG_OK;
 }
 
-// local V=1 site order (T slices) <-> extended lattice (slices + h)
-__global__ void local_to_ext_kernel(Geom loc, Geom ext, int h, const double2 *in, size_t ins, double2 *out,
-                                    size_t outs, int ncomp, int to_ext) {
+// local V=1 site order (Z x T slab) <-> extended lattice (z + hz, t + h)
+__global__ void local_to_ext_kernel(Geom loc, Geom ext, int hz, int h, const double2 *in, size_t ins,
+                                    double2 *out, size_t outs, int ncomp, int to_ext) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < loc.V; i += gridDim.x * blockDim.x) {
     const int par = i >= loc.nh ? 1 : 0;
     int x[4], lex;
     site_coords(loc, par, i - par * loc.nh, x, lex);
-    const int elex = x[0] + ext.L[0] * (x[1] + ext.L[1] * (x[2] + ext.L[2] * (x[3] + h)));
-    const int j = (elex >> 1) + par * ext.nh;  // same parity (h even)
+    const int elex = x[0] + ext.L[0] * (x[1] + ext.L[1] * (x[2] + hz + ext.L[2] * (x[3] + h)));
+    const int j = (elex >> 1) + par * ext.nh;  // same parity (hz, h even)
     for (int c = 0; c < ncomp; c++) {
       if (to_ext)
         out[(size_t)c * outs + j] = in[(size_t)c * ins + i];
@@ -218,8 +314,8 @@ __global__ void unit_diag_kernel(int nl, int V, double2 *u) {
 static int convert(qexstag_domain_s *d, const double2 *in, size_t ins, double2 *out, size_t outs, int ncomp,
                    bool to_ext) {
   const Geom &loc = d->local[0];
-  local_to_ext_kernel<<<grid_for(loc.V), kBlock, 0, stream()>>>(loc, d->ext->g, d->h, in, ins, out, outs, ncomp,
-                                                                to_ext ? 1 : 0);
+  local_to_ext_kernel<<<grid_for(loc.V), kBlock, 0, stream()>>>(loc, d->ext->g, d->hz, d->h, in, ins, out, outs,
+                                                                ncomp, to_ext ? 1 : 0);
   note_launch();
   QS_LAUNCH_CHECK();
   return QEXSTAG_OK;
@@ -231,7 +327,7 @@ static int check_set(qexstag_domain_s *const *ds, int n) {
     if (!ds[k]) return fail(QEXSTAG_ERR_ARG, "domain: null domain");
     if (!ds[k]->connected) return fail(QEXSTAG_ERR_STATE, "domain: not connected to its neighbours");
     if (ds[k]->nl != ds[0]->nl || std::memcmp(ds[k]->gdims, ds[0]->gdims, sizeof ds[0]->gdims) ||
-        ds[k]->nranks != ds[0]->nranks)
+        ds[k]->nranks != ds[0]->nranks || ds[k]->Rz != ds[0]->Rz || ds[k]->hz != ds[0]->hz)
       return fail(QEXSTAG_ERR_ARG, "domain: domains of different lattices in one call");
     if ((ds[k]->comm != nullptr) != (ds[0]->comm != nullptr))
       return fail(QEXSTAG_ERR_ARG, "domain: in-process and NCCL domains in one call");
@@ -306,7 +402,9 @@ static int schur_set(qexstag_domain_s *const *ds, int n, double2 *const *r, doub
   qexstag_domain_s *d0 = ds[0];
   const int sh = (int)slice_half(d0), h = d0->h, T = d0->T;
   const int rho = h / 2;                 // reach of the longest hop
-  const bool overlap = T > 4 * rho;      // some slices need no ghost at all
+  // some slices need no ghost at all (t splits only: with z ghosts every
+  // slice has ghost rows)
+  const bool overlap = d0->hz == 0 && T > 4 * rho;
   QS_CUDA(cudaEventRecord(d0->fork, stream()));
   QS_CUDA(cudaStreamWaitEvent(d0->side, d0->fork, 0));
   if ((rc = exchange(ds, n, x, 3, 0, d0->side))) return rc;
@@ -331,6 +429,15 @@ static int schur_set(qexstag_domain_s *const *ds, int n, double2 *const *r, doub
       if (!rc)
         rc = dslash64_ranges(ds[k]->g, 0, VecD{r[k], g.V}, te, xe, 4.0 * m2, 1.0, -1, h * sh, (h + 2 * rho) * sh,
                              (h + T - 2 * rho) * sh, (h + T) * sh, done);
+    } else if (d0->hz > 0) {
+      // z splits: the intermediate on rows [hz-rho, hz+Z+rho) of slices
+      // [h-rho, h+T+rho), the output on the interior rows of [h, h+T)
+      const int P = (int)row_half(d0), hz = d0->hz, Z = d0->Z;
+      rc = dslash64_rows(ds[k]->g, 1, VecD{t[k] + g.nh, g.V}, xe, CVecD{nullptr, 0}, 0.0, 1.0, +1,
+                         (h - rho) * sh + (hz - rho) * P, T + 2 * rho, (Z + 2 * rho) * P, sh, done);
+      if (!rc)
+        rc = dslash64_rows(ds[k]->g, 0, VecD{r[k], g.V}, te, xe, 4.0 * m2, 1.0, -1, h * sh + hz * P, T, Z * P, sh,
+                           done);
     } else {
       rc = dslash64_ranges(ds[k]->g, 1, VecD{t[k] + g.nh, g.V}, xe, CVecD{nullptr, 0}, 0.0, 1.0, +1,
                            (h - rho) * sh, (h + T + rho) * sh, 0, 0, done);
@@ -343,21 +450,21 @@ static int schur_set(qexstag_domain_s *const *ds, int n, double2 *const *r, doub
   return QEXSTAG_OK;
 }
 
-static int dot_set(qexstag_domain_s *const *ds, int n, double2 *const *a, double2 *const *b, double *out) {
-  std::vector<double> v(n);
-  int rc;
-  for (int k = 0; k < n; k++) {
-    const VecD ia = interior(ds[k], a[k]), ib = interior(ds[k], b[k]);
-    if (a == b)
-      rc = vnorm2(cv(ia), interior_n(ds[k]), &v[k]);
-    else
-      rc = vredot(cv(ia), cv(ib), interior_n(ds[k]), &v[k]);
-    if (rc) return rc;
-  }
-  return allreduce_sum(ds, n, v.data(), out);
-}
-
 // ---- device-resident CG over the domains ----
+
+// which sites of an interior block (t slices [h, h+T), all rows) are not z
+// ghosts: row i / P of the block lies at z = row mod Ze; hz = 0 keeps all
+struct Rows {
+  int P, Ze, hz, Z;
+};
+static Rows rows_of(const qexstag_domain_s *d) {
+  return Rows{(int)row_half(d), d->Z + 2 * d->hz, d->hz, d->Z};
+}
+__device__ __forceinline__ bool in_z(const Rows &w, int i) {
+  if (w.hz == 0) return true;
+  const int z = (i / w.P) % w.Ze;
+  return z >= w.hz && z < w.hz + w.Z;
+}
 
 __global__ void __launch_bounds__(kBlock)
     dm_p_kernel(const double2 *__restrict__ r, double2 *__restrict__ p, int stride, int n, const CgState *st) {
@@ -378,13 +485,14 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// Re <a, b> over one domain's interior into *slot
+// Re <a, b> over one domain's interior into *slot (st may be null)
 __global__ void __launch_bounds__(kBlock)
-    dm_dot_kernel(const double2 *__restrict__ a, const double2 *__restrict__ b, int stride, int n,
+    dm_dot_kernel(const double2 *__restrict__ a, const double2 *__restrict__ b, int stride, int n, Rows w,
                   const CgState *st, double *slot, double *partials, unsigned *ticket) {
-  if (st->done) return;
+  if (st != nullptr && st->done) return;
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (!in_z(w, i)) continue;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const double2 u = a[(size_t)c * stride + i], v = b[(size_t)c * stride + i];
@@ -399,12 +507,13 @@ __global__ void __launch_bounds__(kBlock)
 // x += alpha p, r -= alpha Ap on one domain's interior; |r|^2 into *slot
 __global__ void __launch_bounds__(kBlock)
     dm_xr_kernel(double2 *__restrict__ x, double2 *__restrict__ r, const double2 *__restrict__ p,
-                 const double2 *__restrict__ ap, int stride, int n, const CgState *st, double *slot,
+                 const double2 *__restrict__ ap, int stride, int n, Rows w, const CgState *st, double *slot,
                  double *partials, unsigned *ticket) {
   if (st->done) return;
   const double alpha = st->alpha;
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool keep = in_z(w, i);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const size_t o = (size_t)c * stride + i;
@@ -416,8 +525,10 @@ __global__ void __launch_bounds__(kBlock)
       rv.y = fma(-alpha, av.y, rv.y);
       x[o] = xv;
       r[o] = rv;
-      s = fma(rv.x, rv.x, s);
-      s = fma(rv.y, rv.y, s);
+      if (keep) {
+        s = fma(rv.x, rv.x, s);
+        s = fma(rv.y, rv.y, s);
+      }
     }
   }
   double v[1] = {s}, o[1];
@@ -465,6 +576,32 @@ static int finish_scalar(qexstag_domain_s *const *ds, int n, CgState *st, int wh
   return QEXSTAG_OK;
 }
 
+// Re <a, b> (or |a|^2) over the interiors of the set, summed in rank order
+// and over processes; z ghost rows left out
+static int dot_set(qexstag_domain_s *const *ds, int n, double2 *const *a, double2 *const *b, double *out) {
+  std::vector<double> v(n);
+  int rc;
+  for (int k = 0; k < n; k++) {
+    const VecD ia = interior(ds[k], a[k]), ib = interior(ds[k], b[k]);
+    if (ds[k]->hz > 0) {
+      const int ni = interior_n(ds[k]);
+      dm_dot_kernel<<<std::min(grid_for(ni), kMaxRedBlocks), kBlock, 0, stream()>>>(
+          ia.p, ib.p, ia.stride, ni, rows_of(ds[k]), nullptr, ds[0]->dsum + k, red_partials(), red_tickets());
+      note_launch();
+      QS_LAUNCH_CHECK();
+      QS_CUDA(cudaMemcpyAsync(&v[k], ds[0]->dsum + k, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+      QS_CUDA(cudaStreamSynchronize(stream()));
+      rc = QEXSTAG_OK;
+    } else if (a == b) {
+      rc = vnorm2(cv(ia), interior_n(ds[k]), &v[k]);
+    } else {
+      rc = vredot(cv(ia), cv(ib), interior_n(ds[k]), &v[k]);
+    }
+    if (rc) return rc;
+  }
+  return allreduce_sum(ds, n, v.data(), out);
+}
+
 // one CG iteration (cg.nim:174-240, cpNone) enqueued without a host sync
 static int cg_iteration(qexstag_domain_s *const *ds, int n, double2 *const *xv, double2 *const *rv,
                         double2 *const *pv, double2 *const *ap, double2 *const *tv, double m2, CgState *st) {
@@ -481,7 +618,7 @@ static int cg_iteration(qexstag_domain_s *const *ds, int n, double2 *const *xv, 
     const int ni = interior_n(ds[k]);
     const VecD p = interior(ds[k], pv[k]), a = interior(ds[k], ap[k]);
     dm_dot_kernel<<<std::min(grid_for(ni), kMaxRedBlocks), kBlock, 0, stream()>>>(
-        p.p, a.p, p.stride, ni, st, ds[0]->dsum + k, red_partials(), red_tickets());
+        p.p, a.p, p.stride, ni, rows_of(ds[k]), st, ds[0]->dsum + k, red_partials(), red_tickets());
   }
   note_launch(n);
   QS_LAUNCH_CHECK();
@@ -491,7 +628,7 @@ static int cg_iteration(qexstag_domain_s *const *ds, int n, double2 *const *xv, 
     const VecD x = interior(ds[k], xv[k]), r = interior(ds[k], rv[k]), p = interior(ds[k], pv[k]),
                a = interior(ds[k], ap[k]);
     dm_xr_kernel<<<std::min(grid_for(ni), kMaxRedBlocks), kBlock, 0, stream()>>>(
-        x.p, r.p, p.p, a.p, p.stride, ni, st, ds[0]->dsum + k, red_partials(), red_tickets());
+        x.p, r.p, p.p, a.p, p.stride, ni, rows_of(ds[k]), st, ds[0]->dsum + k, red_partials(), red_tickets());
   }
   note_launch(n);
   QS_LAUNCH_CHECK();
@@ -504,16 +641,23 @@ using namespace qs;
 
 extern "C" {
 
-int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nlinks, qexstag_domain **out) {
+// Rz x Rt ranks (rank = rz + Rz rt); zghost: z ghost rows (qexstag_domain_create_zt)
+static int domain_create(const int global_dims[4], int Rz, int Rt, int rank, int nlinks, bool zghost,
+                         qexstag_domain **out) {
   if (!global_dims || !out) return fail(QEXSTAG_ERR_ARG, "domain_create: null argument");
   if (nlinks != 4 && nlinks != 8) return fail(QEXSTAG_ERR_ARG, "domain_create: nlinks must be 4 or 8");
-  if (nranks < 1 || rank < 0 || rank >= nranks) return fail(QEXSTAG_ERR_ARG, "domain_create: bad rank");
+  const int nranks = Rz * Rt;
+  if (Rz < 1 || Rt < 1 || rank < 0 || rank >= nranks) return fail(QEXSTAG_ERR_ARG, "domain_create: bad rank");
   const int h = nlinks == 8 ? 6 : 2;
-  if (global_dims[3] % nranks) return fail(QEXSTAG_ERR_ARG, "domain_create: L3 is not a multiple of nranks");
-  const int T = global_dims[3] / nranks;
+  if (global_dims[3] % Rt) return fail(QEXSTAG_ERR_ARG, "domain_create: L3 is not a multiple of the t ranks");
+  if (global_dims[2] % Rz) return fail(QEXSTAG_ERR_ARG, "domain_create: L2 is not a multiple of the z ranks");
+  const int T = global_dims[3] / Rt, Z = global_dims[2] / Rz;
   if (T % 2 || T < h || T < 4)
     return fail(QEXSTAG_ERR_ARG, "domain_create: slab thickness must be even, at least 4 and at least the ghost "
                                  "depth (6 fat+Naik, 2 naive)");
+  if (zghost && (Z % 2 || Z < h || Z < 4))
+    return fail(QEXSTAG_ERR_ARG, "domain_create: the z extent of a rank must be even, at least 4 and at least the "
+                                 "ghost depth (6 fat+Naik, 2 naive)");
   int rc = runtime_ready();
   if (rc) return rc;
   qexstag_domain_s *d = new (std::nothrow) qexstag_domain_s;
@@ -521,11 +665,17 @@ int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nl
   std::memcpy(d->gdims, global_dims, sizeof d->gdims);
   d->nranks = nranks;
   d->rank = rank;
+  d->Rz = Rz;
+  d->Rt = Rt;
+  d->rz = rank % Rz;
+  d->rt = rank / Rz;
   d->nl = nlinks;
   d->h = h;
   d->T = T;
-  const int edims[4] = {global_dims[0], global_dims[1], global_dims[2], T + 2 * h};
-  const int ldims[4] = {global_dims[0], global_dims[1], global_dims[2], T};
+  d->Z = Z;
+  d->hz = zghost ? h : 0;
+  const int edims[4] = {global_dims[0], global_dims[1], Z + 2 * d->hz, T + 2 * h};
+  const int ldims[4] = {global_dims[0], global_dims[1], Z, T};
   qexstag_layout *le = nullptr, *ll = nullptr;
   if ((rc = qexstag_layout_create(edims, &le)) || (rc = qexstag_layout_create(ldims, &ll))) {
     if (le) qexstag_layout_destroy(le);
@@ -570,6 +720,16 @@ int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nl
   return QEXSTAG_OK;
 }
 
+int qexstag_domain_create(const int global_dims[4], int nranks, int rank, int nlinks, qexstag_domain **out) {
+  return domain_create(global_dims, 1, nranks, rank, nlinks, false, out);
+}
+
+int qexstag_domain_create_zt(const int global_dims[4], const int grid[2], int rank, int nlinks,
+                             qexstag_domain **out) {
+  if (!grid) return fail(QEXSTAG_ERR_ARG, "domain_create_zt: null grid");
+  return domain_create(global_dims, grid[0], grid[1], rank, nlinks, true, out);
+}
+
 int qexstag_domain_destroy(qexstag_domain *d) {
   if (!d) return QEXSTAG_OK;
   if (d->comm && nccl().ok) nccl().commDestroy(d->comm);
@@ -588,7 +748,9 @@ int qexstag_domain_destroy(qexstag_domain *d) {
 
 int qexstag_domain_local_dims(const qexstag_domain *d, int dims[4]) {
   if (!d || !dims) return fail(QEXSTAG_ERR_ARG, "domain_local_dims: null argument");
-  for (int k = 0; k < 3; k++) dims[k] = d->gdims[k];
+  dims[0] = d->gdims[0];
+  dims[1] = d->gdims[1];
+  dims[2] = d->Z;
   dims[3] = d->T;
   return QEXSTAG_OK;
 }
@@ -598,13 +760,17 @@ int qexstag_domain_connect_local(qexstag_domain *const *doms, int n) {
   for (int k = 0; k < n; k++) {
     if (!doms[k] || doms[k]->nranks != n || doms[k]->rank != k)
       return fail(QEXSTAG_ERR_ARG, "domain_connect_local: pass every rank's domain, in rank order");
-    if (doms[k]->nl != doms[0]->nl || std::memcmp(doms[k]->gdims, doms[0]->gdims, sizeof doms[0]->gdims))
+    if (doms[k]->nl != doms[0]->nl || std::memcmp(doms[k]->gdims, doms[0]->gdims, sizeof doms[0]->gdims) ||
+        doms[k]->Rz != doms[0]->Rz || doms[k]->hz != doms[0]->hz)
       return fail(QEXSTAG_ERR_ARG, "domain_connect_local: domains of different lattices");
   }
   for (int k = 0; k < n; k++) {
-    doms[k]->up = doms[(k + 1) % n];
-    doms[k]->down = doms[(k + n - 1) % n];
-    doms[k]->connected = true;
+    qexstag_domain_s *d = doms[k];
+    d->up = doms[rank_of(d, d->rz, d->rt + 1)];
+    d->down = doms[rank_of(d, d->rz, d->rt - 1)];
+    d->zup = doms[rank_of(d, d->rz + 1, d->rt)];
+    d->zdown = doms[rank_of(d, d->rz - 1, d->rt)];
+    d->connected = true;
   }
   return QEXSTAG_OK;
 }
@@ -717,6 +883,9 @@ int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x,
     QS_CUDA(cudaMemsetAsync(xv[k], 0, bytes, stream()));
     QS_CUDA(cudaMemsetAsync(pv[k], 0, bytes, stream()));
     QS_CUDA(cudaMemsetAsync(rv[k], 0, bytes, stream()));
+    // sites the sweeps do not write (z ghost rows) stay zero
+    QS_CUDA(cudaMemsetAsync(ap[k], 0, bytes, stream()));
+    QS_CUDA(cudaMemsetAsync(tv[k], 0, bytes, stream()));
     const int ni = interior_n(d);
     if ((rc = vcopy(interior(d, rv[k]), cv(interior(d, bv[k])), ni)) ||
         (rc = vcopy(interior(d, pv[k]), cv(interior(d, bv[k])), ni)))

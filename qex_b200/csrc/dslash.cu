@@ -39,8 +39,10 @@ struct DslashArgs64 {
   unsigned *ticket;
   double *dot_out;
   // output sites: [k0, k0 + n1) then [k2, k2 + nsites - n1) of the parity
-  // block (the whole block: k0 = k2 = 0, n1 = nsites = nh)
+  // block (the whole block: k0 = k2 = 0, n1 = nsites = nh); with rowlen > 0
+  // instead nsites / rowlen runs of rowlen sites, pitch apart, from k0
   int k0, n1, k2, nsites;
+  int rowlen, pitch;
 };
 
 template <int NL, int HOP, int INIT, int RED>
@@ -54,7 +56,13 @@ __global__ void __launch_bounds__(kBlock) dslash64_kernel(const DslashArgs64 A) 
   const size_t out_base = (size_t)A.po * nh;
   double dot = 0.0;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < A.nsites; j += gridDim.x * blockDim.x) {
-    const int k = j < A.n1 ? A.k0 + j : A.k2 + (j - A.n1);
+    int k;
+    if (A.rowlen > 0) {
+      const int q = j / A.rowlen;
+      k = A.k0 + q * A.pitch + (j - q * A.rowlen);
+    } else {
+      k = j < A.n1 ? A.k0 + j : A.k2 + (j - A.n1);
+    }
     int x[4], lex;
     site_coords(g, A.po, k, x, lex);
     double2 acc[3];
@@ -197,6 +205,7 @@ int dslash64(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, C
   A.dot_out = dot_out;
   A.k0 = A.k2 = 0;
   A.n1 = A.nsites = g.nh;
+  A.rowlen = A.pitch = 0;
   int grid = grid_for(g.nh, kBlock, 6);
   if (red != kRedNone && grid > kMaxRedBlocks) grid = kMaxRedBlocks;
   int rc = (gl->nl == 8) ? dispatch64<8>(A, hop, init, red, grid)
@@ -234,6 +243,43 @@ int dslash64_ranges(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVec
   A.n1 = k1 - k0;
   A.k2 = k2;
   A.nsites = (k1 - k0) + (k3 - k2);
+  if (A.nsites == 0) return QEXSTAG_OK;
+  const int init = xs.p ? 1 : 0;
+  const int rc = (gl->nl == 8) ? dispatch64<8>(A, hop, init, kRedNone, grid_for(A.nsites, kBlock, 6))
+                               : dispatch64<4>(A, hop, init, kRedNone, grid_for(A.nsites, kBlock, 6));
+  if (rc) return rc;
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
+}
+
+// One half sweep over nrun runs of rowlen sites of parity po, pitch apart,
+// from k0 (a block of z rows in each of a range of t slices): out = b xs +
+// c (2D) xin with hop sign hop, no reduction; skipped once *done is set.
+int dslash64_rows(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, double b, double c, int hop,
+                  int k0, int nrun, int rowlen, int pitch, const int *done) {
+  const Geom &g = gl->l->g;
+  if (k0 < 0 || nrun < 0 || rowlen < 0 || rowlen > pitch ||
+      (nrun > 0 && (long)k0 + (long)(nrun - 1) * pitch + rowlen > g.nh))
+    return fail(QEXSTAG_ERR_ARG, "dslash64_rows: site runs outside the parity block");
+  DslashArgs64 A;
+  std::memset(&A, 0, sizeof(A));
+  A.g = g;
+  A.po = po;
+  A.u = gl->u64;
+  A.xin = xin.p;
+  A.istride = xin.stride;
+  A.xs = xs.p;
+  A.sstride = xs.stride;
+  A.out = out.p;
+  A.ostride = out.stride;
+  A.b = b;
+  A.c = c;
+  A.done = done;
+  A.k0 = k0;
+  A.rowlen = rowlen;
+  A.pitch = pitch;
+  A.nsites = nrun * rowlen;
+  A.n1 = A.nsites;
   if (A.nsites == 0) return QEXSTAG_OK;
   const int init = xs.p ? 1 : 0;
   const int rc = (gl->nl == 8) ? dispatch64<8>(A, hop, init, kRedNone, grid_for(A.nsites, kBlock, 6))

@@ -84,6 +84,8 @@ int schur64(const qexstag_links_s *g, int par, VecD r, CVecD x, VecD t, double m
             double *dot_out = nullptr);
 int dslash64_ranges(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, double b, double c,
                     int hop, int k0, int k1, int k2, int k3, const int *done);
+int dslash64_rows(const qexstag_links_s *gl, int po, VecD out, CVecD xin, CVecD xs, double b, double c, int hop,
+                  int k0, int nrun, int rowlen, int pitch, const int *done);
 
 // ---- blas.cu ----
 int aos_to_soa(const double *aos, double2 *soa, int n, int stride, int ncomp);

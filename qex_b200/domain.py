@@ -23,12 +23,18 @@ def _arr(ptrs):
 
 
 class DomainSet:
-    """The domains this process holds: ranks[0..] of an nranks split."""
+    """The domains this process holds: ranks[0..] of an nranks split along t,
+    or, with grid = (Rz, Rt), of an Rz x Rt split along t and z (nranks =
+    Rz Rt, rank = rz + Rz rt)."""
 
-    def __init__(self, global_dims, nranks: int, nlinks: int, ranks=None, nccl_id: bytes | None = None):
+    def __init__(self, global_dims, nranks: int, nlinks: int, ranks=None, nccl_id: bytes | None = None,
+                 grid=None):
         S.init(0)
         self.lib = L.load()
         self.gdims = tuple(int(d) for d in global_dims)
+        self.grid = (1, nranks) if grid is None else (int(grid[0]), int(grid[1]))
+        if grid is not None and self.grid[0] * self.grid[1] != nranks:
+            raise ValueError("grid does not hold nranks ranks")
         self.nranks = nranks
         self.nl = nlinks
         self.ranks = list(range(nranks)) if ranks is None else list(ranks)
@@ -36,7 +42,11 @@ class DomainSet:
         dims = (C.c_int * 4)(*self.gdims)
         for r in self.ranks:
             h = C.c_void_p()
-            L.check(self.lib.qexstag_domain_create(dims, nranks, r, nlinks, C.byref(h)), "domain_create")
+            if grid is None:
+                rc = self.lib.qexstag_domain_create(dims, nranks, r, nlinks, C.byref(h))
+            else:
+                rc = self.lib.qexstag_domain_create_zt(dims, (C.c_int * 2)(*self.grid), r, nlinks, C.byref(h))
+            L.check(rc, "domain_create")
             self.handles.append(h)
         ld = (C.c_int * 4)()
         L.check(self.lib.qexstag_domain_local_dims(self.handles[0], ld), "domain_local_dims")
@@ -52,7 +62,8 @@ class DomainSet:
         self.gidx = []
         for r in self.ranks:
             g = c.copy()
-            g[:, 3] += r * self.ldims[3]
+            g[:, 2] += (r % self.grid[0]) * self.ldims[2]
+            g[:, 3] += (r // self.grid[0]) * self.ldims[3]
             self.gidx.append(F.index_of(self.gdims, g))
 
     def _set(self):
@@ -120,6 +131,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dims", default="32,32,32,32")
     ap.add_argument("--ranks", default="1,2")
+    ap.add_argument("--grids", default="", help="splits along t and z as RzxRt, e.g. 2x1,2x2")
     ap.add_argument("--mass", type=float, default=0.01)
     ap.add_argument("--r2req", type=float, default=1e-20)
     a = ap.parse_args()
@@ -143,6 +155,17 @@ def main():
             d.solveEE(y, b, a.mass, sp)
         out[f"ranks_{R}"] = {"slab": d.ldims[3], "iterations": sp.iterations, "seconds": sp.seconds,
                              "true_r2": sp.r2, "max_diff_vs_one_lattice": float(np.abs(y - x).max())}
+        del d
+    for spec in (v for v in a.grids.split(",") if v):
+        Rz, Rt = (int(v) for v in spec.split("x"))
+        d = DomainSet(dims, Rz * Rt, 8, grid=(Rz, Rt))
+        d.set_links(g)
+        for _ in range(2):
+            y = np.zeros_like(b)
+            sp = S.SolverParams(r2req=a.r2req)
+            d.solveEE(y, b, a.mass, sp)
+        out[f"grid_{Rz}x{Rt}"] = {"local": d.ldims, "iterations": sp.iterations, "seconds": sp.seconds,
+                                  "true_r2": sp.r2, "max_diff_vs_one_lattice": float(np.abs(y - x).max())}
         del d
     print(json.dumps(out))
 

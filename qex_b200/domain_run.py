@@ -1,7 +1,7 @@
 """A CG solve decomposed along t, one rank per GPU (NCCL), under torchrun:
 
   python -m torch.distributed.run --nproc-per-node N --master-addr 127.0.0.1 \
-      -m qex_b200.domain_run --dims 32,32,32,64
+      -m qex_b200.domain_run --dims 32,32,32,64 [--zranks Rz]
 
 Each rank builds the same synthetic fat+Naik field and source (seeded),
 keeps its slab, rank 0 makes the NCCL id and broadcasts it over the
@@ -23,6 +23,8 @@ def main():
     ap.add_argument("--dims", default="16,16,16,32")
     ap.add_argument("--mass", type=float, default=0.05)
     ap.add_argument("--r2req", type=float, default=1e-20)
+    ap.add_argument("--zranks", type=int, default=0,
+                    help="split along t and z with this many ranks along z (0: along t only)")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -36,7 +38,8 @@ def main():
     dims = tuple(int(v) for v in a.dims.split(","))
     obj = [DD.nccl_unique_id() if rank == 0 else None]
     dist.broadcast_object_list(obj, src=0)
-    d = DD.DomainSet(dims, world, 8, ranks=[rank], nccl_id=obj[0])
+    grid = (a.zranks, world // a.zranks) if a.zranks > 0 else None
+    d = DD.DomainSet(dims, world, 8, ranks=[rank], nccl_id=obj[0], grid=grid)
     g = F.fat_naik_links(dims, 21)
     b = F.even_source(dims, 31)
     d.set_links(g)

@@ -114,3 +114,87 @@ def test_torchrun_one_rank_per_gpu(cuda, tmp_path):
     line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1]
     res = json.loads(line)
     assert res["ranks"] == 1 and res["true_r2"] <= 1e-20 * 1.0001 and res["status"] == 0
+
+
+# splits along t and z: (dims, nlinks, [(Rz, Rt), ...]); (1, 1) keeps z ghosts
+# and exchanges them with itself
+ZT_CASES = [((4, 4, 12, 12), 8, [(1, 1), (2, 1), (1, 2), (2, 2)]),
+            ((4, 4, 8, 8), 4, [(1, 1), (2, 2)]),
+            ((4, 4, 16, 8), 4, [(4, 2)])]
+
+
+@pytest.mark.parametrize("dims,nl,grids", ZT_CASES)
+def test_zt_schur_matches_single_lattice(cuda, dims, nl, grids):
+    """Every rank of an Rz x Rt split in one process: even sites of the Schur
+    operator bit-exact against the single lattice (the corner ghosts reach
+    the second half sweep through the Naik hops), odd sites untouched."""
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 5) if nl == 8 else F.naive_links(dims, 0.4, 5)
+    x = F.gaussian_vector(V, 6)
+    ref = x.copy()
+    S.Staggered(S.Layout(dims), g).stagD2ee(ref, x, 0.04)
+    for Rz, Rt in grids:
+        d = DD.DomainSet(dims, Rz * Rt, nl, grid=(Rz, Rt))
+        assert d.ldims == (dims[0], dims[1], dims[2] // Rz, dims[3] // Rt)
+        d.set_links(g)
+        r = x.copy()
+        d.stagD2ee(r, x, 0.04)
+        assert np.array_equal(r[: V // 2], ref[: V // 2]), (Rz, Rt)
+        assert np.array_equal(r[V // 2:], x[V // 2:])
+
+
+@pytest.mark.parametrize("dims,nl,grids", ZT_CASES)
+def test_zt_cg_matches_oracle(cuda, dims, nl, grids):
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 7) if nl == 8 else F.naive_links(dims, 0.4, 7)
+    b = F.even_source(dims, 8)
+    o = O.Oracle(dims, g)
+    xo = o.vec()
+    its_o, _ = o.cg(0, xo, b, 0.01, 1e-20)
+    for Rz, Rt in grids:
+        d = DD.DomainSet(dims, Rz * Rt, nl, grid=(Rz, Rt))
+        d.set_links(g)
+        x = np.zeros_like(b)
+        sp = S.SolverParams(r2req=1e-20)
+        d.solveEE(x, b, 0.1, sp)
+        assert abs(sp.iterations - its_o) <= 2, (Rz, Rt, sp.iterations, its_o)
+        assert sp.r2 <= 1e-20 * 1.0001
+        assert rel(x[: V // 2], xo[: V // 2]) < 1e-8
+        assert not np.any(x[V // 2:])
+
+
+def test_zt_nccl_self_exchange(cuda):
+    """A 1 x 1 grid over an NCCL communicator of size 1: the z faces are
+    packed, sent to the rank itself and unpacked; results equal the
+    in-process path's."""
+    dims = (4, 4, 8, 8)
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 9)
+    x = F.gaussian_vector(V, 10)
+    local = DD.DomainSet(dims, 1, 8, grid=(1, 1))
+    local.set_links(g)
+    viaccl = DD.DomainSet(dims, 1, 8, nccl_id=DD.nccl_unique_id(), grid=(1, 1))
+    viaccl.set_links(g)
+    a, b = x.copy(), x.copy()
+    local.stagD2ee(a, x, 0.09)
+    viaccl.stagD2ee(b, x, 0.09)
+    assert np.array_equal(a, b)
+    ref = x.copy()
+    S.Staggered(S.Layout(dims), g).stagD2ee(ref, x, 0.09)
+    assert np.array_equal(a[: V // 2], ref[: V // 2])
+    src = F.even_source(dims, 11)
+    ya, yb = np.zeros_like(src), np.zeros_like(src)
+    spa, spb = S.SolverParams(r2req=1e-18), S.SolverParams(r2req=1e-18)
+    local.solveEE(ya, src, 0.2, spa)
+    viaccl.solveEE(yb, src, 0.2, spb)
+    assert spa.iterations == spb.iterations and np.array_equal(ya, yb)
+
+
+def test_zt_errors(cuda):
+    lib = L.load()
+    import ctypes as C
+    h = C.c_void_p()
+    dims = (C.c_int * 4)(4, 4, 12, 12)
+    assert lib.qexstag_domain_create_zt(dims, (C.c_int * 2)(4, 1), 0, 8, C.byref(h)) == L.ERR_ARG  # Z = 3
+    assert lib.qexstag_domain_create_zt(dims, (C.c_int * 2)(5, 1), 0, 8, C.byref(h)) == L.ERR_ARG  # 12 % 5
+    assert lib.qexstag_domain_create_zt(dims, (C.c_int * 2)(2, 2), 4, 8, C.byref(h)) == L.ERR_ARG  # rank 4 of 4
