@@ -22,6 +22,16 @@ def _arr(ptrs):
     return (C.c_void_p * len(ptrs))(*ptrs)
 
 
+def rank_sites(global_dims, local_dims, grid, rank: int) -> np.ndarray:
+    """Global V=1 index of each site of rank's local lattice, in the local
+    V=1 order: rank = rz + Rz rt holds z rows [rz Z, (rz+1) Z) of slices
+    [rt T, (rt+1) T)."""
+    g = F.coords(tuple(local_dims))
+    g[:, 2] += (rank % grid[0]) * local_dims[2]
+    g[:, 3] += (rank // grid[0]) * local_dims[3]
+    return F.index_of(tuple(global_dims), g)
+
+
 class DomainSet:
     """The domains this process holds: ranks[0..] of an nranks split along t,
     or, with grid = (Rz, Rt), of an Rz x Rt split along t and z (nranks =
@@ -58,13 +68,7 @@ class DomainSet:
             for h in self.handles:
                 L.check(self.lib.qexstag_domain_connect_nccl(h, buf), "domain_connect_nccl")
         # global index of each local site, per rank
-        c = F.coords(self.ldims)
-        self.gidx = []
-        for r in self.ranks:
-            g = c.copy()
-            g[:, 2] += (r % self.grid[0]) * self.ldims[2]
-            g[:, 3] += (r // self.grid[0]) * self.ldims[3]
-            self.gidx.append(F.index_of(self.gdims, g))
+        self.gidx = [rank_sites(self.gdims, self.ldims, self.grid, r) for r in self.ranks]
 
     def _set(self):
         return _arr([h.value for h in self.handles])

@@ -70,3 +70,19 @@ def test_two_phase_exchange_fills_every_ghost(gdims, Rz, Rt, h):
     complete, rows_ok = _plan(gdims, Rz, Rt, h)
     assert complete
     assert rows_ok
+
+
+@pytest.mark.parametrize("gdims,grid", [((4, 4, 8, 8), (1, 2)), ((4, 4, 12, 12), (2, 2)), ((4, 4, 16, 8), (4, 2)),
+                                        ((8, 4, 6, 16), (1, 4))])
+def test_rank_sites_partition_the_lattice(gdims, grid):
+    """The ranks' sites (DomainSet's split of global fields) cover every
+    global site once, and a local site's parity is its global parity."""
+    from qex_b200.domain import rank_sites
+    ldims = (gdims[0], gdims[1], gdims[2] // grid[0], gdims[3] // grid[1])
+    V, Vl = F.volume(gdims), F.volume(ldims)
+    owned = np.concatenate([rank_sites(gdims, ldims, grid, r) for r in range(grid[0] * grid[1])])
+    assert np.array_equal(np.sort(owned), np.arange(V))
+    for r in range(grid[0] * grid[1]):
+        gi = rank_sites(gdims, ldims, grid, r)
+        # V=1 order: the first half of each lattice is even
+        assert np.all((gi[: Vl // 2] < V // 2)) and np.all(gi[Vl // 2:] >= V // 2)
