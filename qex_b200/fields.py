@@ -71,6 +71,21 @@ def rand_tah(n: int, rng: np.random.Generator) -> np.ndarray:
     return m
 
 
+def su3_generators() -> np.ndarray:
+    """The 8 traceless anti-Hermitian generators i lambda_a (Gell-Mann
+    matrices lambda_a), shape (8, 3, 3)."""
+    lam = np.zeros((8, 3, 3), dtype=np.complex128)
+    lam[0][0, 1] = lam[0][1, 0] = 1
+    lam[1][0, 1], lam[1][1, 0] = -1j, 1j
+    lam[2][0, 0], lam[2][1, 1] = 1, -1
+    lam[3][0, 2] = lam[3][2, 0] = 1
+    lam[4][0, 2], lam[4][2, 0] = -1j, 1j
+    lam[5][1, 2] = lam[5][2, 1] = 1
+    lam[6][1, 2], lam[6][2, 1] = -1j, 1j
+    lam[7] = np.diag([1, 1, -2]) / np.sqrt(3)
+    return 1j * lam
+
+
 def exp_ah(t: np.ndarray, eps: float | np.ndarray = 1.0) -> np.ndarray:
     """exp(eps * t) for anti-Hermitian t (..., 3, 3)."""
     h = -1j * t  # Hermitian

@@ -34,18 +34,22 @@ def test_force_is_the_derivative_of_the_action(dims, rect):
     f = O.gauge_force(dims, u, plaq, rect)
     # the action is ~1e4: its rounding (~1e-11) over 2 eps bounds the
     # difference from below, the eps^2 truncation from above
+    # along all 8 generators on 64 seeded (site, direction) entries
     eps = 1e-4
-    for _ in range(8):
-        mu, x = int(rng.integers(0, 4)), int(rng.integers(0, V))
-        T = F.rand_tah(1, rng)[0]
-        vals = []
-        for e in (eps, -eps):
-            up = u.copy()
-            up[mu, x] = scipy.linalg.expm(e * T) @ u[mu, x]
-            vals.append(O.gauge_action(dims, up, plaq, rect))
-        fd = (vals[0] - vals[1]) / (2 * eps)
-        an = np.trace(np.conj(T).T @ f[mu, x]).real
-        assert abs(fd - an) < 2e-6 * max(1.0, abs(an)), (mu, x, fd, an)
+    entries = set()
+    while len(entries) < 64:
+        entries.add((int(rng.integers(0, 4)), int(rng.integers(0, V))))
+    gens = F.su3_generators()
+    for mu, x in sorted(entries):
+        for a, T in enumerate(gens):
+            vals = []
+            for e in (eps, -eps):
+                up = u.copy()
+                up[mu, x] = scipy.linalg.expm(e * T) @ u[mu, x]
+                vals.append(O.gauge_action(dims, up, plaq, rect))
+            fd = (vals[0] - vals[1]) / (2 * eps)
+            an = np.trace(np.conj(T).T @ f[mu, x]).real
+            assert abs(fd - an) < 2e-6 * max(1.0, abs(an)), (mu, x, a, fd, an)
     # traceless anti-Hermitian
     assert np.abs(f + np.conj(np.swapaxes(f, -1, -2))).max() < 1e-13
     assert np.abs(np.trace(f, axis1=-2, axis2=-1)).max() < 1e-13

@@ -247,20 +247,6 @@ def _action(o, phi, m):
     return np.vdot(phi[: V // 2], y[: V // 2]).real
 
 
-def _su3_generators():
-    """The 8 anti-Hermitian traceless generators i lambda_a (Gell-Mann)."""
-    lam = np.zeros((8, 3, 3), dtype=np.complex128)
-    lam[0][0, 1] = lam[0][1, 0] = 1
-    lam[1][0, 1], lam[1][1, 0] = -1j, 1j
-    lam[2][0, 0], lam[2][1, 1] = 1, -1
-    lam[3][0, 2] = lam[3][2, 0] = 1
-    lam[4][0, 2], lam[4][2, 0] = -1j, 1j
-    lam[5][1, 2] = lam[5][2, 1] = 1
-    lam[6][1, 2], lam[6][2, 1] = -1j, 1j
-    lam[7] = np.diag([1, 1, -2]) / np.sqrt(3)
-    return 1j * lam
-
-
 @pytest.mark.parametrize("naik", [False, True])
 def test_force_finite_difference(naik):
     """dS/deps for U_k(x) -> exp(eps T_a) U_k(x) equals ReTr[T_a f_k(x)^dagger]/8
@@ -281,7 +267,7 @@ def test_force_finite_difference(naik):
     entries = set()
     while len(entries) < 64:
         entries.add((int(rng.integers(0, g.shape[0])), int(rng.integers(0, V))))
-    gens = _su3_generators()
+    gens = F.su3_generators()
     eps = 1e-5
     for k, s in sorted(entries):
         for a, T in enumerate(gens):
