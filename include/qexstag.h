@@ -183,7 +183,10 @@ int qexstag_stagD2oo(qexstag_links *g, double *r, const double *x, double m2, in
    65536 (larger lattices return QEXSTAG_ERR_ARG); every GPU that loads the
    library holds it until exit.  All calls on a device share that array:
    calls that overlap on the GPU race.  The first call on a device looks up
-   the array's address; make it before any stream capture. */
+   the array's address; make it before any stream capture.  The address is
+   kept until qexstag_finalize; a host that resets the device calls
+   qexstag_finalize before the reset (the module may load at another address
+   afterwards), and the next call looks the address up again. */
 int qexstag_stagD2ee_noalloc(qexstag_links *g, double *r, const double *x, double m2);
 
 /* ---- solvers (src/physics/stagSolve.nim, src/solvers/cg.nim, cgm.nim) ---- */

@@ -54,6 +54,10 @@ def lib():
             "or_norm2": (D, [P, I, P]),
             "or_redot": (D, [P, I, P, P]),
             "or_cg_xx": (I, [P, I, P, P, D, D, I, DP]),
+            "or_cg_begin": (P, [P, I, P, P, D, D]),
+            "or_cg_run": (I, [P, I]),
+            "or_cg_converged": (I, [P]),
+            "or_cg_end": (I, [P, DP]),
             "or_solveXX": (I, [P, I, P, P, D, D, I, DP]),
             "or_eoReconstruct": (None, [P, P, P, D]),
             "or_solve": (I, [P, P, P, D, D, I, DP]),
@@ -166,6 +170,11 @@ class Oracle:
         r2 = C.c_double()
         its = lib().or_cg_xx(self.ctx, parity, _p(x), _p(b), m2, r2req, maxits, C.byref(r2))
         return its, r2.value
+
+    def cg_steps(self, parity, x, b, m2, r2req):
+        """The same CG as cg(), run in pieces: returns a CgRun whose
+        run(n) performs up to n more iterations."""
+        return CgRun(self, parity, x, b, m2, r2req)
 
     def solveXX(self, parity, r, x, m, r2req, maxits=100000):
         r2 = C.c_double()
@@ -341,3 +350,35 @@ def link_update(u, p, eps: float):
     p = np.ascontiguousarray(p, dtype=np.complex128)
     lib().or_link_update(u.size // 9, _p(u), _p(p), eps)
     return u
+
+
+class CgRun:
+    """One oracle CG solve (or_cg_begin / or_cg_run / or_cg_end), run a
+    bounded number of iterations at a time.  Holds references to the
+    operator, solution and source for its lifetime."""
+
+    def __init__(self, o: Oracle, parity, x, b, m2, r2req):
+        self.o, self.x, self.b = o, x, b
+        self.state = lib().or_cg_begin(o.ctx, parity, _p(x), _p(b), m2, r2req)
+        self.iterations = 0
+
+    def run(self, n: int) -> int:
+        """Up to n more iterations; returns the iterations done so far."""
+        self.iterations = lib().or_cg_run(self.state, self.iterations + int(n))
+        return self.iterations
+
+    @property
+    def converged(self) -> bool:
+        return bool(lib().or_cg_converged(self.state))
+
+    def end(self):
+        """Frees the state; returns (iterations, |r|^2/|b|^2)."""
+        r2 = C.c_double()
+        its = lib().or_cg_end(self.state, C.byref(r2))
+        self.state = None
+        return its, r2.value
+
+    def __del__(self):
+        if getattr(self, "state", None):
+            lib().or_cg_end(self.state, None)
+            self.state = None

@@ -371,50 +371,96 @@ double or_redot(void *ctx, int parity, const double *x, const double *y) {
 /*   A y = b, A = stagD2xx(m2); x enters as the initial guess.          */
 /* ------------------------------------------------------------------ */
 
-int or_cg_xx(void *ctx, int parity, double *x, const double *b, double m2,
-             double r2req, int maxits, double *r2_out) {
-  OCtx *c = (OCtx *)ctx;
+/* The solve is split into begin / run / end so that a caller can run it in
+   bounded pieces (the CPU baseline times one whole solve as a sequence of
+   steps); or_cg_xx is begin, one run to maxits, end. */
+typedef struct {
+  OCtx *c;
+  int parity;
   long i0, i1;
-  subset_range(c, parity, &i0, &i1);
+  double *x, *r, *p, *Ap;
+  double m2, b2, r2, rzo, r2stop;
+  int itn;
+} OrCg;
+
+void *or_cg_begin(void *ctx, int parity, double *x, const double *b, double m2, double r2req) {
+  OCtx *c = (OCtx *)ctx;
+  OrCg *s = (OrCg *)calloc(1, sizeof(OrCg));
   long n = 6 * c->V;
-  double *r = (double *)calloc(n, sizeof(double));
-  double *p = (double *)calloc(n, sizeof(double));
-  double *Ap = (double *)calloc(n, sizeof(double));
-  double b2 = norm2_sub(c, parity, b);
-  double r2 = 0, rzo = 1.0;
-  int itn = 0;
-  if (b2 == 0.0) {
-    for (long i = 6 * i0; i < 6 * i1; i++) x[i] = 0;
-    r2 = 0;
+  s->c = c;
+  s->parity = parity;
+  subset_range(c, parity, &s->i0, &s->i1);
+  s->x = x;
+  s->m2 = m2;
+  s->r = (double *)calloc(n, sizeof(double));
+  s->p = (double *)calloc(n, sizeof(double));
+  s->Ap = (double *)calloc(n, sizeof(double));
+  s->b2 = norm2_sub(c, parity, b);
+  s->r2 = 0;
+  s->rzo = 1.0;
+  s->itn = 0;
+  if (s->b2 == 0.0) {
+    for (long i = 6 * s->i0; i < 6 * s->i1; i++) x[i] = 0;
   } else {
-    or_stagD2ee_par(c, parity, Ap, x, m2);
-    for (long i = 6 * i0; i < 6 * i1; i++) { r[i] = b[i] - Ap[i]; p[i] = 0; }
-    r2 = norm2_sub(c, parity, r);
+    or_stagD2ee_par(c, parity, s->Ap, x, m2);
+    for (long i = 6 * s->i0; i < 6 * s->i1; i++) { s->r[i] = b[i] - s->Ap[i]; s->p[i] = 0; }
+    s->r2 = norm2_sub(c, parity, s->r);
   }
-  double r2stop = r2req * b2;
-  while (itn < maxits && r2 > r2stop) {
-    double rz = r2;
-    double beta = rz / rzo;
-    rzo = rz;
-    if (itn == 0) {
+  s->r2stop = r2req * s->b2;
+  return s;
+}
+
+/* Runs iterations until itn reaches maxits (a total, not a count for this
+   call) or the residual meets the target; returns itn. */
+int or_cg_run(void *state, int maxits) {
+  OrCg *s = (OrCg *)state;
+  OCtx *c = s->c;
+  const long i0 = s->i0, i1 = s->i1;
+  double *x = s->x, *r = s->r, *p = s->p, *Ap = s->Ap;
+  while (s->itn < maxits && s->r2 > s->r2stop) {
+    double rz = s->r2;
+    double beta = rz / s->rzo;
+    s->rzo = rz;
+    if (s->itn == 0) {
       for (long i = 6 * i0; i < 6 * i1; i++) p[i] = r[i];
     } else {
       for (long i = 6 * i0; i < 6 * i1; i++) p[i] = r[i] + beta * p[i];
     }
-    itn++;
-    or_stagD2ee_par(c, parity, Ap, p, m2);
-    double pAp = redot_sub(c, parity, p, Ap);
+    s->itn++;
+    or_stagD2ee_par(c, s->parity, Ap, p, s->m2);
+    double pAp = redot_sub(c, s->parity, p, Ap);
     double alpha = rz / pAp;
 #pragma omp parallel for schedule(static)
     for (long i = 6 * i0; i < 6 * i1; i++) {
       x[i] += alpha * p[i];
       r[i] -= alpha * Ap[i];
     }
-    r2 = norm2_sub(c, parity, r);
+    s->r2 = norm2_sub(c, s->parity, r);
   }
-  if (r2_out) *r2_out = (b2 > 0) ? r2 / b2 : 0.0;
-  free(r); free(p); free(Ap);
+  return s->itn;
+}
+
+/* 1 once the iterated residual meets the target. */
+int or_cg_converged(void *state) {
+  OrCg *s = (OrCg *)state;
+  return !(s->r2 > s->r2stop);
+}
+
+/* Frees the state; returns the iterations and *r2_out = |r|^2/|b|^2. */
+int or_cg_end(void *state, double *r2_out) {
+  OrCg *s = (OrCg *)state;
+  int itn = s->itn;
+  if (r2_out) *r2_out = (s->b2 > 0) ? s->r2 / s->b2 : 0.0;
+  free(s->r); free(s->p); free(s->Ap);
+  free(s);
   return itn;
+}
+
+int or_cg_xx(void *ctx, int parity, double *x, const double *b, double m2,
+             double r2req, int maxits, double *r2_out) {
+  void *s = or_cg_begin(ctx, parity, x, b, m2, r2req);
+  or_cg_run(s, maxits);
+  return or_cg_end(s, r2_out);
 }
 
 /* solveXXInternal for the FP64 QEX backend (stagSolve.nim:90-161 and

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 from pathlib import Path
 
@@ -35,7 +36,7 @@ def _headers():
 def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     hdr_time = max((h.stat().st_mtime for h in _headers()), default=0.0)
-    objs = []
+    objs, jobs = [], []
     for src in _sources():
         obj = OBJ / (src.stem + ".o")
         objs.append(obj)
@@ -46,12 +47,20 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError(f"nvcc failed on {src.name}")
-        if ptxas_info or verbose:
-            sys.stderr.write(r.stderr)
+        jobs.append((src, cmd))
+
+    def compile_one(job):
+        src, cmd = job
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per source file, as many at a time as there are host cores
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for src, r in pool.map(compile_one, jobs):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError(f"nvcc failed on {src.name}")
+            if ptxas_info or verbose:
+                sys.stderr.write(r.stderr)
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]

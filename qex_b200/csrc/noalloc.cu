@@ -20,7 +20,10 @@
 // but two calls that run at the same time on the GPU (different streams, or
 // different host threads) race on it.  The first call on each device looks up
 // the array's device address (cudaGetSymbolAddress), so make that first
-// call before any stream capture.
+// call before any stream capture.  The address is cached per device until
+// qexstag_finalize, which forgets it: a host that resets the device
+// (cudaDeviceReset) calls qexstag_finalize first, because after a reset the
+// module can load at another address; the next call then looks it up again.
 #include <mutex>
 
 #include "lib.cuh"
@@ -51,6 +54,13 @@ static int noalloc_tmp(int dev, double2 **out) {
   }
   *out = g_noalloc_ptr[dev];
   return QEXSTAG_OK;
+}
+
+// forget the cached address on device dev (qexstag_finalize)
+void noalloc_forget(int dev) {
+  if (dev < 0 || dev >= kNoAllocDevices) return;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  g_noalloc_ptr[dev] = nullptr;
 }
 
 }  // namespace qs

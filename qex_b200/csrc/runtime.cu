@@ -8,6 +8,8 @@
 
 namespace qs {
 
+void noalloc_forget(int dev);  // noalloc.cu
+
 namespace {
 thread_local std::string g_last_error = "no error";
 thread_local cudaStream_t g_stream = nullptr;
@@ -109,6 +111,7 @@ int qexstag_init(int device) {
 
 int qexstag_finalize(void) {
   int d = qs::current_device();
+  qs::noalloc_forget(d);
   std::lock_guard<std::mutex> lock(qs::g_mutex);
   qs::DeviceRuntime &r = qs::g_dev[d];
   if (!r.ready) return QEXSTAG_OK;

@@ -213,6 +213,29 @@ def test_solvers_meet_residual(naik):
     assert res <= r2req
 
 
+def test_cg_in_steps_equals_one_call():
+    """The CPU baseline runs one oracle CG in bounded pieces; the pieces
+    give the iterations and solution of a single call (OpenMP sums are not
+    bitwise reproducible from run to run, so the solution is compared to
+    1e-8)."""
+    dims = (4, 4, 4, 8)
+    V = F.volume(dims)
+    o = O.Oracle(dims, _links(dims, True))
+    b = F.gaussian_vector(V, 11)
+    m2 = 0.01
+    x1 = o.vec()
+    its1, r21 = o.cg(0, x1, b, m2, 1e-20)
+    x2 = o.vec()
+    run = o.cg_steps(0, x2, b, m2, 1e-20)
+    steps = 0
+    while not run.converged:
+        run.run(7)
+        steps += 1
+    its2, r22 = run.end()
+    assert abs(its2 - its1) <= 1 and steps == -(-its2 // 7)
+    assert r22 <= 1e-20 and rel(x2, x1) < 1e-8
+
+
 def test_multishift_matches_single():
     dims = (4, 4, 4, 4)
     V = F.volume(dims)

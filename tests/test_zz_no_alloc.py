@@ -5,7 +5,10 @@ whose pool allocator already holds the device memory, or one that cannot
 take cudaMalloc's device-wide synchronisation mid-pipeline).  Called through
 the C ABI it must give what qexstag_stagD2ee gives for device fields, on two
 calls in a row (the calls share one static temporary), without lowering the
-device's free memory, and must reject lattices beyond its static limit.
+device's free memory, and must reject lattices beyond its static limit.  Both
+entry points run the same FP64 half-sweep kernel on every site, so their
+results are compared bit for bit; the oracle is the CPU reference, within
+the Dslash tolerance.
 This file is collected last so that a failure here does not hide the others.
 """
 import ctypes as C
@@ -13,6 +16,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from qex_b200 import _lib as L
 from qex_b200 import fields as F
 from qex_b200 import stag as S
@@ -50,10 +54,16 @@ def test_noalloc_schur_matches_stagD2ee(cuda, dims, naik):
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free_before
     want = S.to_host_vector(ref)[:h]
-    scale = np.abs(want).max()
+    xo = S.to_host_vector(x)
+    xo[h:] = 0
+    o = O.Oracle(dims, g)
+    ro = o.vec()
+    o.stagD2ee(ro, xo, m2)
+    scale = np.abs(ro[:h]).max()
     for r in outs:
         got = S.to_host_vector(r)
-        assert np.abs(got[:h] - want).max() / scale < TOL
+        assert np.array_equal(got[:h], want)  # same kernel, same sites: bit-identical
+        assert np.abs(got[:h] - ro[:h]).max() / scale < TOL
         assert not np.any(got[h:])  # odd sites untouched
 
 
@@ -68,3 +78,26 @@ def test_noalloc_rejects_lattices_beyond_its_limit(cuda):
     rc = lib.qexstag_stagD2ee_noalloc(s.handle, _ptr(r), _ptr(x), 0.01)
     assert rc == L.ERR_ARG
     assert "65536" in lib.qexstag_last_error().decode()
+
+
+def test_noalloc_after_finalize(cuda):
+    """qexstag_finalize forgets the array's address; the next call looks it
+    up again and still matches stagD2ee bit for bit."""
+    torch = cuda
+    dims = (8, 8, 8, 8)
+    V = F.volume(dims)
+    g = F.naive_links(dims, 0.3, 9)
+    s = S.Staggered(S.Layout(dims), S.to_device_links(g))
+    x = S.to_device_vector(F.gaussian_vector(V, 12))
+    ref = torch.zeros_like(x)
+    s.stagD2ee(ref, x, 0.04)
+    lib = L.load()
+    r = torch.zeros_like(x)
+    assert lib.qexstag_stagD2ee_noalloc(s.handle, _ptr(r), _ptr(x), 0.04) == L.OK
+    torch.cuda.synchronize()
+    assert lib.qexstag_finalize() == L.OK
+    r2 = torch.zeros_like(x)
+    rc = lib.qexstag_stagD2ee_noalloc(s.handle, _ptr(r2), _ptr(x), 0.04)
+    assert rc == L.OK, lib.qexstag_last_error().decode()
+    torch.cuda.synchronize()
+    assert torch.equal(r2, ref) and torch.equal(r, ref)
