@@ -24,6 +24,20 @@ from . import stag as S
 SHAPES = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (8, 8, 8, 16)]
 
 
+def problem_set(n=64, seed=2024):
+    """The seeded problem set: per problem (dims, phased links (4, V, 3, 3),
+    mass, even source), host arrays in QEX's V=1 order."""
+    rng = np.random.default_rng(seed)
+    probs = []
+    for i in range(n):
+        dims = SHAPES[int(rng.integers(0, len(SHAPES)))]
+        eps = float(rng.uniform(0.1, 0.5))
+        m = float(rng.uniform(0.02, 0.2))
+        g = F.apply_phases(dims, F.gauge_warm(dims, eps, 1000 + i))
+        probs.append((dims, g, m, F.even_source(dims, 2000 + i)))
+    return probs
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=64)
@@ -31,16 +45,11 @@ def main():
     a = ap.parse_args()
     import torch
     S.init(0)
-    rng = np.random.default_rng(2024)
     t0 = time.perf_counter()
     stags, bs, ms, dims_list = [], [], [], []
-    for i in range(a.n):
-        dims = SHAPES[int(rng.integers(0, len(SHAPES)))]
-        eps = float(rng.uniform(0.1, 0.5))
-        m = float(rng.uniform(0.02, 0.2))
-        g = F.apply_phases(dims, F.gauge_warm(dims, eps, 1000 + i))
+    for dims, g, m, b in problem_set(a.n):
         stags.append(S.Staggered(S.Layout(dims), S.to_device_links(g)))
-        bs.append(S.to_device_vector(F.even_source(dims, 2000 + i)))
+        bs.append(S.to_device_vector(b))
         ms.append(m)
         dims_list.append(dims)
     setup = time.perf_counter() - t0

@@ -22,6 +22,11 @@ from . import fields as F
 from . import stag as S
 
 
+def shifts(nshift=12):
+    """sigma_k = 10^(-4 + 4k/(nshift-1)): log-spaced from 1e-4 to 1."""
+    return [10.0 ** (-4 + 4 * k / (nshift - 1)) for k in range(nshift)]
+
+
 def run(dims, nrhs, nshift, mass, r2req, sloppies):
     import torch
     S.init(0)
@@ -30,7 +35,7 @@ def run(dims, nrhs, nshift, mass, r2req, sloppies):
     g = F.fat_naik_links(dims, 21)
     s = S.Staggered(S.Layout(dims), S.to_device_links(g))
     del g
-    sig = [10.0 ** (-4 + 4 * k / (nshift - 1)) for k in range(nshift)]
+    sig = shifts(nshift)
     bs = [S.to_device_vector(F.even_source(dims, 100 + j)) for j in range(nrhs)]
     ys = [[torch.zeros((3, V), dtype=torch.complex128, device="cuda") for _ in sig] for _ in bs]
     out = {"dims": dims, "nrhs": nrhs, "nshift": nshift, "mass": mass, "r2req": r2req,

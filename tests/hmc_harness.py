@@ -1,4 +1,6 @@
-"""HMC glue for the staggered fermion force (QEX src/hmc/hmcAction.nim).
+"""Test harness: an eager-torch HMC around the library's fermion force
+(QEX src/hmc/hmcAction.nim), used by the GPU tests as an independent
+restatement to check the device MD driver qex_b200/md.py against.
 
 The fermion parts go through the library: the pseudofermion heatbath
 (D(-m) psi, hmcAction.nim:794-823), the action (solve, 825-849), the force
@@ -24,8 +26,8 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import fields as F
-from . import stag as S
+from qex_b200 import fields as F
+from qex_b200 import stag as S
 
 
 def dagger(m):
@@ -322,41 +324,3 @@ def thermalize(lat, U, beta, ntraj, tau=1.0, nsteps=20, seed=11):
         if dh <= 0 or rng.random() < np.exp(-dh):
             U, acc = U1, acc + 1
     return U, acc
-
-
-def main():
-    """Config 4: 16^4, beta 5.6, one pseudofermion (m = 0.05), tau = 1,
-    20 leapfrog steps, reversibility check (after --therm pure-gauge
-    thermalisation trajectories from a warm start)."""
-    import argparse
-    import json
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--dims", default="16,16,16,16")
-    ap.add_argument("--beta", type=float, default=5.6)
-    ap.add_argument("--mass", type=float, default=0.05)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--tau", type=float, default=1.0)
-    ap.add_argument("--naive", action="store_true")
-    ap.add_argument("--hisq", action="store_true", help="HISQ-smeared fermion operator and force")
-    ap.add_argument("--therm", type=int, default=10)
-    a = ap.parse_args()
-    dims = tuple(int(v) for v in a.dims.split(","))
-    S.init(0)
-    lat = Lattice(dims)
-    U0 = torch.from_numpy(F.gauge_warm(dims, 0.3, 41)).to("cuda")
-    import time
-    t0 = time.perf_counter()
-    U0, acc = thermalize(lat, U0, a.beta, a.therm)
-    t1 = time.perf_counter()
-    out = trajectory_with_reversal(lat, U0, a.beta, a.mass, None if a.naive else -1.0 / 24.0, a.tau, a.steps,
-                                   hisq=a.hisq)
-    out["fermion"] = "hisq" if a.hisq else ("naive" if a.naive else "thin fat+Naik")
-    out["seconds"] = time.perf_counter() - t1
-    out["thermalization"] = {"trajectories": a.therm, "accepted": acc, "seconds": t1 - t0}
-    out["plaquette"] = -out.pop("plaquette_action") / (a.beta / 3.0) / (6 * lat.V * 3)
-    out["dims"] = dims
-    print(json.dumps(out))
-
-
-if __name__ == "__main__":
-    main()

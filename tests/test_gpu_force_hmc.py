@@ -100,7 +100,7 @@ def test_hmc_trajectory_reversible(cuda):
     the square of the step (halving it divides dH by ~4) and the reversed
     trajectory returns to the start."""
     torch = cuda
-    from qex_b200 import hmc
+    import hmc_harness as hmc
     dims = (8, 8, 8, 8)
     lat = hmc.Lattice(dims)
     U0 = torch.from_numpy(F.gauge_warm(dims, 0.3, 41)).to("cuda")
@@ -117,7 +117,7 @@ def test_hmc_force_matches_finite_difference(cuda):
     """The MD force (Wilson + fermion through the Naik chain rule) against a
     central difference of the potential along su(3) generators."""
     torch = cuda
-    from qex_b200 import hmc
+    import hmc_harness as hmc
     dims = (4, 4, 4, 8)
     lat = hmc.Lattice(dims)
     U = torch.from_numpy(F.gauge_warm(dims, 0.3, 5)).to("cuda")
@@ -147,7 +147,7 @@ def test_hisq_hmc_force_matches_finite_difference(cuda):
     fat7, projectU, fat7 + Naik) against a central difference of the
     potential along su(3) generators on the thin links."""
     torch = cuda
-    from qex_b200 import hmc
+    import hmc_harness as hmc
     dims = (4, 4, 4, 8)
     lat = hmc.Lattice(dims)
     U = torch.from_numpy(F.gauge_warm(dims, 0.3, 6)).to("cuda")
@@ -175,7 +175,7 @@ def test_hisq_hmc_trajectory_reversible(cuda):
     """HISQ trajectories (QEX's tgenerichmchisq shape): dH falls as the square
     of the step and the reversed trajectory returns to the start."""
     torch = cuda
-    from qex_b200 import hmc
+    import hmc_harness as hmc
     dims = (8, 8, 8, 8)
     lat = hmc.Lattice(dims)
     U0 = torch.from_numpy(F.gauge_warm(dims, 0.3, 43)).to("cuda")

@@ -79,7 +79,8 @@ def test_momenta_heatbath(cuda):
 
 def test_pure_gauge_md_matches_torch_hmc(cuda):
     torch = cuda
-    from qex_b200 import hmc, md
+    import hmc_harness as hmc
+    from qex_b200 import md
     dims = (8, 8, 8, 8)
     lay = S.Layout(dims)
     lat = hmc.Lattice(dims)
@@ -104,7 +105,8 @@ def test_md_with_fermion_matches_torch_hmc(cuda, hisq):
     operator written as one-link-only smearing.  Same U, p and phi as
     qex_b200/hmc.py's trajectory; dH agrees and the trajectory reverses."""
     torch = cuda
-    from qex_b200 import hmc, md
+    import hmc_harness as hmc
+    from qex_b200 import md
     dims = (8, 8, 8, 8)
     lay = S.Layout(dims)
     lat = hmc.Lattice(dims)

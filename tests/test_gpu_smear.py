@@ -245,7 +245,6 @@ def test_hisq_force_finite_differences(cuda):
     links; along W -> exp(t T_a) W on one thin link, dS/dt = Re Tr[T_a
     f^dag]/8 (f carries QEX's factor 4 in psi and S_QEX = 2 S)."""
     torch = cuda
-    from qex_b200.force_check import gell_mann
     dims = (4, 4, 4, 6)
     V = F.volume(dims)
     h = V // 2
@@ -259,7 +258,7 @@ def test_hisq_force_finite_differences(cuda):
     coef = SM.newHISQ()
     f = np.empty_like(g)
     sm.force(stag, coef, g, f, phi, m, S.SolverParams(r2req=1e-26))
-    T = gell_mann()
+    T = F.su3_generators()
     rng = np.random.default_rng(17)
     eps = 1e-5
     worst, scale = 0.0, 0.0
