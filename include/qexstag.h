@@ -147,12 +147,37 @@ int qexstag_links_destroy(qexstag_links *g);
    so an HMC update of U is seen by the next solve; with device copies the
    caller calls this after changing the links. */
 int qexstag_links_update(qexstag_links *g, const double *links, int mem);
-/* QEX's rephase (src/physics/stagD.nim:106-114): multiply the handle's links
-   by the staggered phases [8,9,11,0] and the antiperiodic time boundary
-   signs (setBC, src/gauge/gaugeUtils.nim:133-140; for three-hop long links
-   the product of their three one-hop signs).  Applying it twice restores
-   the links, so it folds phases in and out; reduced copies are rebuilt. */
+/* QEX's rephase(s) (src/physics/stagD.nim:106-114), literally: setBC
+   (src/gauge/gaugeUtils.nim:133-140) negates field 3 of the list on the last
+   time slice and stagPhase (stagD.nim:560-571) multiplies fields 0..3 by
+   eta_0..eta_3 (phases [8,9,11,0]).  For a naive list these are the four
+   directions.  For a fat+Naik list, as in QEX, only the first four fields
+   [fat_0, long_0, fat_1, long_1] change (eta_0..eta_3, BC on long_1); use
+   qexstag_links_rephase_all to phase every field by its own direction.
+   Applying it twice restores the links; reduced copies are rebuilt. */
 int qexstag_links_rephase(qexstag_links *g);
+/* Every field of the list by its own direction and hop (no single QEX call
+   does this): one-hop links of direction mu get eta_mu(x), and -1 on the
+   last time slice for mu = 3; three-hop long links get eta_mu(x), and -1
+   when the hop crosses the time boundary (the product of their three
+   one-hop signs), as QEX's HISQ path folds them (stagPhase and setBC before
+   smearing, src/hmc/hmcAction.nim:540-555).  Applying it twice restores the
+   links; reduced copies are rebuilt. */
+int qexstag_links_rephase_all(qexstag_links *g);
+/* Links in MILC order, as QUDA's MILC interface takes them
+   (QUDA_MILC_GAUGE_ORDER, which QEX's QUDA wrapper fills from Staggered.g at
+   src/quda/qudaWrapperImpl.nim:134-139, 205-245): host arrays with the four
+   directions of a site together, fat[V][4][3][3][2] and, for a fat+Naik
+   operator, lng[V][4][3][3][2] (lng == NULL: a naive operator), sites in
+   the V=1 order above, phases folded in.  The handle is the one
+   qexstag_links_create makes from QEX's list [fat_0, long_0, ..., fat_3,
+   long_3] (or [U_0 .. U_3]). */
+int qexstag_links_create_milc(qexstag_layout *l, const double *fat, const double *lng, double long_coeff,
+                              qexstag_links **out);
+int qexstag_links_update_milc(qexstag_links *g, const double *fat, const double *lng);
+/* Copy the handle's FP64 links out in MILC order (the inverse of
+   qexstag_links_create_milc). */
+int qexstag_links_get_milc(qexstag_links *g, double *fat, double *lng);
 /* 1 when the handle uses 12-real long links in its reduced precisions. */
 int qexstag_links_recon12(const qexstag_links *g);
 

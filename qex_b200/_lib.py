@@ -106,6 +106,10 @@ SIGNATURES = {
     "qexstag_links_recon12": (I, [P]),
     "qexstag_links_update": (I, [P, P, I]),
     "qexstag_links_rephase": (I, [P]),
+    "qexstag_links_rephase_all": (I, [P]),
+    "qexstag_links_create_milc": (I, [P, P, P, D, C.POINTER(C.c_void_p)]),
+    "qexstag_links_update_milc": (I, [P, P, P]),
+    "qexstag_links_get_milc": (I, [P, P, P]),
     "qexstag_stagD2": (I, [P, I, P, P, D, D, I]),
     "qexstag_stagD": (I, [P, I, P, P, D, D, D, I]),
     "qexstag_D": (I, [P, P, P, D, I]),

@@ -1,6 +1,7 @@
 // api.cu -- the extern "C" entry points declared in include/qexstag.h:
 // argument checking, staging of host fields (QEX V=1 array-of-structs) to the
 // device layout and back, and dispatch to the kernels.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -21,7 +22,7 @@ int solve_multishift(qexstag_links_s *g, int nmass, double2 *const *xs, const do
 int apply_D(qexstag_links_s *g, double2 *r, const double2 *x, double m, double sc);
 int stagD_par(qexstag_links_s *g, int par, double2 *r, const double2 *x, double m, double sc,
               double a);
-int rephase_links(qexstag_links_s *g);
+int rephase_links(qexstag_links_s *g, bool literal);
 
 int Workspace::get(int slot, size_t bytes, void **out) {
   auto it = bufs.find(slot);
@@ -303,6 +304,58 @@ static int upload_links(qexstag_links_s *g, const double *links, int mem) {
   }
   return QEXSTAG_OK;
 }
+// MILC order (QUDA_MILC_GAUGE_ORDER): a site's four directions together,
+// double[V][4][3][3][2] per list.  kind 0: the naive list (slot mu), 1: fat
+// links of a fat+Naik list (slot 2 mu), 2: its long links (slot 2 mu + 1).
+// Sites [s0, s0 + n) pass through aos, n * 4 * 9 double2.
+__global__ void milc_soa_kernel(double2 *__restrict__ aos, double2 *__restrict__ soa, int V, int s0, int n, int kind,
+                                int to_soa) {
+  const int ss = kind == 0 ? 1 : 2, so = kind == 2 ? 1 : 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * 36; t += gridDim.x * blockDim.x) {
+    const int i = t / 36, r = t - i * 36, mu = r / 9, c = r - mu * 9;
+    double2 *d = soa + ((size_t)(mu * ss + so) * 9 + c) * V + s0 + i;
+    if (to_soa)
+      *d = aos[t];
+    else
+      aos[t] = *d;
+  }
+}
+
+static int milc_transfer(qexstag_links_s *g, double *host, int kind, bool up) {
+  const Geom &geo = g->l->g;
+  const size_t per = sizeof(double2) * 9 * (size_t)geo.V;  // staging: V/4 sites of 4 directions
+  void *aos;
+  int rc = g->ws.get(kSlotAos, per, &aos);
+  if (rc) return rc;
+  const int chunk = geo.V / 4;
+  for (int s0 = 0; s0 < geo.V; s0 += chunk) {
+    const int n = std::min(chunk, geo.V - s0);
+    double *h = host + (size_t)s0 * 4 * 18;
+    const size_t bytes = sizeof(double2) * 36 * (size_t)n;
+    if (up) QS_CUDA(cudaMemcpyAsync(aos, h, bytes, cudaMemcpyHostToDevice, stream()));
+    milc_soa_kernel<<<grid_for((long)n * 36), kBlock, 0, stream()>>>((double2 *)aos, g->u64, geo.V, s0, n, kind,
+                                                                        up ? 1 : 0);
+    note_launch();
+    QS_LAUNCH_CHECK();
+    if (!up) {
+      QS_CUDA(cudaMemcpyAsync(h, aos, bytes, cudaMemcpyDeviceToHost, stream()));
+      QS_CUDA(cudaStreamSynchronize(stream()));  // the staging buffer is reused by the next chunk
+    }
+  }
+  return QEXSTAG_OK;
+}
+
+static int upload_links_milc(qexstag_links_s *g, const double *fat, const double *lng) {
+  int rc = milc_transfer(g, const_cast<double *>(fat), g->nl == 8 ? 1 : 0, true);
+  if (!rc && g->nl == 8) rc = milc_transfer(g, const_cast<double *>(lng), 2, true);
+  return rc;
+}
+
+static int download_links_milc(qexstag_links_s *g, double *fat, double *lng) {
+  int rc = milc_transfer(g, fat, g->nl == 8 ? 1 : 0, false);
+  if (!rc && g->nl == 8) rc = milc_transfer(g, lng, 2, false);
+  return rc;
+}
 }  // namespace qs
 
 extern "C" {
@@ -361,7 +414,72 @@ int qexstag_links_update(qexstag_links *g, const double *links, int mem) {
 int qexstag_links_rephase(qexstag_links *g) {
   int rc;
   if ((rc = check_links(g))) return rc;
-  if ((rc = rephase_links(g))) return rc;
+  if ((rc = rephase_links(g, true))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_rephase_all(qexstag_links *g) {
+  int rc;
+  if ((rc = check_links(g))) return rc;
+  if ((rc = rephase_links(g, false))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_create_milc(qexstag_layout *l, const double *fat, const double *lng, double long_coeff,
+                              qexstag_links **out) {
+  if (!l || !fat || !out) return fail(QEXSTAG_ERR_ARG, "links_create_milc: null argument");
+  int rc;
+  if ((rc = runtime_ready())) return rc;
+  if (long_coeff == 0.0 || !std::isfinite(long_coeff))
+    return fail(QEXSTAG_ERR_ARG, "links_create_milc: long_coeff must be finite and nonzero");
+  const int nl = lng ? 8 : 4;
+  qexstag_links_s *g = new (std::nothrow) qexstag_links_s;
+  if (!g) return fail(QEXSTAG_ERR_ALLOC, "links_create_milc: out of host memory");
+  g->l = l;
+  g->nl = nl;
+  g->long_coeff = long_coeff;
+  const size_t per = sizeof(double2) * 9 * (size_t)l->g.V;
+  cudaError_t e = cudaMalloc(&g->u64, per * nl);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete g;
+    return fail(QEXSTAG_ERR_ALLOC, "links_create_milc: device allocation failed");
+  }
+  if ((rc = upload_links_milc(g, fat, lng)) || (rc = build_low_links(g))) {
+    g->ws.release();
+    free_low_links(g->low);
+    cudaFree(g->u64);
+    delete g;
+    return rc;
+  }
+  e = cudaStreamSynchronize(stream());
+  if (e != cudaSuccess) return cuda_fail(e, "links_create_milc");
+  *out = g;
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_update_milc(qexstag_links *g, const double *fat, const double *lng) {
+  int rc;
+  if ((rc = check_links(g))) return rc;
+  if (!fat || ((g->nl == 8) != (lng != nullptr)))
+    return fail(QEXSTAG_ERR_ARG, "links_update_milc: fat is null, or lng is given for a naive handle "
+                                 "or missing for a fat+Naik handle");
+  if ((rc = upload_links_milc(g, fat, lng))) return rc;
+  free_low_links(g->low);
+  if ((rc = build_low_links(g))) return rc;
+  QS_CUDA(cudaStreamSynchronize(stream()));
+  return QEXSTAG_OK;
+}
+
+int qexstag_links_get_milc(qexstag_links *g, double *fat, double *lng) {
+  int rc;
+  if ((rc = check_links(g))) return rc;
+  if (!fat || ((g->nl == 8) != (lng != nullptr)))
+    return fail(QEXSTAG_ERR_ARG, "links_get_milc: fat is null, or lng is given for a naive handle "
+                                 "or missing for a fat+Naik handle");
+  if ((rc = download_links_milc(g, fat, lng))) return rc;
   QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
 }

@@ -1,11 +1,22 @@
-// phases.cu -- staggered phases and boundary signs on the device link copy
-// (QEX's rephase: setBC then stagPhase, src/physics/stagD.nim:106-114,
-// 560-571, src/gauge/gaugeUtils.nim:133-140).  Multiplying by the signs
-// twice restores the links, so the same call folds phases in and out.
-// One-hop links of direction mu get eta_mu(x) (phases [8,9,11,0]) and -1 on
-// the last time slice for mu = 3; three-hop long links get eta_mu(x) and -1
-// when the hop crosses the time boundary (the product of their three
-// one-hop signs).
+// phases.cu -- staggered phases and boundary signs on the device link copy.
+// Multiplying by the signs twice restores the links, so the same call folds
+// phases in and out.
+//
+// rephase_links(g, literal = true) is QEX's rephase exactly (setBC then
+// stagPhase, src/physics/stagD.nim:106-114, 560-571,
+// src/gauge/gaugeUtils.nim:133-140): both act on the first four fields of the
+// operator's list, whatever its length -- field k gets eta_k(x) (phases
+// [8,9,11,0]) and field 3 gets -1 on the last time slice.  For a naive list
+// those are the four directions.  For newStag3's interleaved list
+// [fat_0, long_0, fat_1, long_1, ...] QEX's call therefore phases fat_0,
+// long_0, fat_1, long_1 with eta_0..eta_3, puts the boundary sign on long_1
+// and leaves the rest unchanged; the literal form reproduces that.
+//
+// rephase_links(g, literal = false) phases every field of the list by its own
+// direction and hop, which QEX has no single call for: one-hop links of
+// direction mu get eta_mu(x) and -1 on the last time slice for mu = 3;
+// three-hop long links get eta_mu(x) and -1 when the hop crosses the time
+// boundary (the product of their three one-hop signs).
 #include "lib.cuh"
 #include "lowprec.cuh"
 
@@ -14,6 +25,8 @@ namespace qs {
 int build_low_links(qexstag_links_s *g);
 void free_low_links(LowLinks &low);
 
+// NL fields of the list are rephased, field l as direction Hop<NL>::mu(l)
+// with hop Hop<NL>::len(l) (NL = 4: fields 0-3 as directions 0-3, one hop)
 template <int NL>
 __global__ void rephase_kernel(Geom g, double2 *__restrict__ u) {
   const size_t V = (size_t)g.V;
@@ -38,10 +51,10 @@ __global__ void rephase_kernel(Geom g, double2 *__restrict__ u) {
   }
 }
 
-int rephase_links(qexstag_links_s *g) {
+int rephase_links(qexstag_links_s *g, bool literal) {
   const Geom &geo = g->l->g;
   const int grid = grid_for((long)geo.V * g->nl, kBlock, 8);
-  if (g->nl == 8)
+  if (g->nl == 8 && !literal)
     rephase_kernel<8><<<grid, kBlock, 0, stream()>>>(geo, g->u64);
   else
     rephase_kernel<4><<<grid, kBlock, 0, stream()>>>(geo, g->u64);

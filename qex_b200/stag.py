@@ -183,10 +183,60 @@ class Staggered:
         ptr, mem = _ptr(links)
         L.check(self._lib.qexstag_links_update(self.handle, ptr, mem), "links_update")
 
+    @classmethod
+    def from_milc(cls, layout: Layout, fat: np.ndarray, lng: np.ndarray | None = None,
+                  long_coeff: float = 1.0) -> "Staggered":
+        """Operator from links in MILC order, as QUDA's MILC interface takes
+        them (qudaWrapperImpl.nim:205-245): host complex128 arrays of shape
+        (V, 4, 3, 3), the four directions of a site together; lng None for a
+        naive operator."""
+        self = cls.__new__(cls)
+        self.l = layout
+        self._lib = layout._lib
+        fat = cls._milc_array(layout, fat)
+        lp = None if lng is None else cls._milc_array(layout, lng)
+        h = C.c_void_p()
+        L.check(self._lib.qexstag_links_create_milc(layout.handle, C.c_void_p(fat.ctypes.data),
+                                                    None if lp is None else C.c_void_p(lp.ctypes.data),
+                                                    float(long_coeff), C.byref(h)), "links_create_milc")
+        self.handle = h
+        self.nlinks = 4 if lng is None else 8
+        return self
+
+    @staticmethod
+    def _milc_array(layout, a):
+        if not isinstance(a, np.ndarray) or a.dtype != np.complex128 or not a.flags.c_contiguous \
+                or a.shape != (layout.V, 4, 3, 3):
+            raise ValueError("MILC-order links must be C-contiguous complex128 arrays of shape (V, 4, 3, 3)")
+        return a
+
+    def update_links_milc(self, fat: np.ndarray, lng: np.ndarray | None = None) -> None:
+        fat = self._milc_array(self.l, fat)
+        lp = None if lng is None else self._milc_array(self.l, lng)
+        L.check(self._lib.qexstag_links_update_milc(self.handle, C.c_void_p(fat.ctypes.data),
+                                                    None if lp is None else C.c_void_p(lp.ctypes.data)),
+                "links_update_milc")
+
+    def links_milc(self):
+        """The operator's FP64 links in MILC order: (fat, long) arrays of
+        shape (V, 4, 3, 3); long is None for a naive operator."""
+        fat = np.empty((self.l.V, 4, 3, 3), dtype=np.complex128)
+        lng = np.empty_like(fat) if self.nlinks == 8 else None
+        L.check(self._lib.qexstag_links_get_milc(self.handle, C.c_void_p(fat.ctypes.data),
+                                                 None if lng is None else C.c_void_p(lng.ctypes.data)),
+                "links_get_milc")
+        return fat, lng
+
     def rephase(self) -> None:
-        """QEX's rephase: fold the staggered phases and boundary signs into
-        (or out of) the operator's links."""
+        """QEX's rephase(s) exactly: setBC + stagPhase on the first four
+        fields of the link list (for a fat+Naik list: fat_0, long_0, fat_1,
+        long_1, as QEX's own call does)."""
         L.check(self._lib.qexstag_links_rephase(self.handle), "links_rephase")
+
+    def rephase_all(self) -> None:
+        """Fold the staggered phases and boundary signs into (or out of)
+        every field of the list by its own direction and hop."""
+        L.check(self._lib.qexstag_links_rephase_all(self.handle), "links_rephase_all")
 
     @property
     def recon12(self) -> bool:

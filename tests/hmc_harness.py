@@ -148,7 +148,7 @@ class StaggeredFermion:
         # force is its qexstag_hisq_force (smearing chain rule included)
         self.hisq = hisq
         if hisq:
-            from . import smear as SM
+            from qex_b200 import smear as SM
             self.sm = SM.Smear(self.lay)
             self.coef = SM.newHISQ()
             self.smear_seconds = 0.0

@@ -128,8 +128,9 @@ def test_argument_errors(cuda):
 
 @pytest.mark.parametrize("naik", [False, True])
 def test_rephase_on_device(cuda, naik):
-    """rephase of unphased links gives the operator of the phased links
-    (oracle's setBC + stagPhase); a second rephase restores them."""
+    """Phasing every field of unphased links gives the operator of the
+    phased links (oracle's setBC + stagPhase per direction and hop); a
+    second call restores them.  For naive links this is QEX's rephase."""
     dims = (8, 4, 6, 8)
     V = F.volume(dims)
     if naik:
@@ -139,7 +140,8 @@ def test_rephase_on_device(cuda, naik):
     else:
         raw = F.gauge_warm(dims, 0.3, 4)
     s = S.Staggered(S.Layout(dims), raw)
-    s.rephase()
+    flip = s.rephase_all if naik else s.rephase
+    flip()
     o = O.Oracle(dims, O.apply_phases(dims, raw))
     x = F.gaussian_vector(V, 9)
     a, b = np.zeros_like(x), np.zeros_like(x)
@@ -148,8 +150,64 @@ def test_rephase_on_device(cuda, naik):
     assert rel(a, b) < TOL
     if naik:
         assert s.recon12
-    s.rephase()
+    flip()
     o2 = O.Oracle(dims, raw)
     o2.D(b, x, 0.1)
     s.D(a, x, 0.1)
     assert rel(a, b) < TOL
+
+
+def test_rephase_fat_naik_is_qex_literal(cuda):
+    """QEX's rephase(s) on newStag3's list acts on its first four fields
+    only (setBC on field 3, stagPhase eta_k on field k, stagD.nim:106-114):
+    fat_0, long_0, fat_1, long_1 change, the rest do not."""
+    dims = (8, 4, 6, 8)
+    V = F.volume(dims)
+    rng = np.random.default_rng(6)
+    raw = F.interleave(F.fat_from_su3(F.warm_su3(4 * V, 0.3, rng), rng).reshape(4, V, 3, 3),
+                       F.warm_su3(4 * V, 0.3, rng).reshape(4, V, 3, 3))
+    want = raw.copy()
+    want[:4] = O.apply_phases(dims, np.ascontiguousarray(raw[:4]))  # fields 0-3 as directions 0-3
+    s = S.Staggered(S.Layout(dims), raw)
+    s.rephase()
+    t = S.Staggered(S.Layout(dims), want)
+    x = F.gaussian_vector(V, 10)
+    a, b = np.zeros_like(x), np.zeros_like(x)
+    s.D(a, x, 0.1)
+    t.D(b, x, 0.1)
+    assert np.array_equal(a, b)
+    fat, lng = s.links_milc()
+    assert np.array_equal(fat, np.ascontiguousarray(np.moveaxis(want[0::2], 0, 1)))
+    assert np.array_equal(lng, np.ascontiguousarray(np.moveaxis(want[1::2], 0, 1)))
+
+
+@pytest.mark.parametrize("naik", [False, True])
+def test_links_milc_order(cuda, naik):
+    """Links in MILC order (QUDA's MILC gauge order, qudaWrapperImpl.nim:
+    205-245) give the operator of QEX's list bit for bit, and come back out
+    unchanged."""
+    dims = (8, 4, 6, 8)
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 12) if naik else F.naive_links(dims, 0.3, 12)
+    fat = np.ascontiguousarray(np.moveaxis(g[0::2] if naik else g, 0, 1))
+    lng = np.ascontiguousarray(np.moveaxis(g[1::2], 0, 1)) if naik else None
+    lay = S.Layout(dims)
+    s = S.Staggered(lay, g)
+    m = S.Staggered.from_milc(lay, fat, lng)
+    assert m.nlinks == s.nlinks and m.recon12 == s.recon12
+    x = F.gaussian_vector(V, 13)
+    a, b = np.zeros_like(x), np.zeros_like(x)
+    s.D(a, x, 0.07)
+    m.D(b, x, 0.07)
+    assert np.array_equal(a, b)
+    f2, l2 = m.links_milc()
+    assert np.array_equal(f2, fat) and (l2 is None or np.array_equal(l2, lng))
+    f3, l3 = s.links_milc()  # QEX-ordered upload, MILC-ordered download
+    assert np.array_equal(f3, fat) and (l3 is None or np.array_equal(l3, lng))
+    g2 = F.fat_naik_links(dims, 14) if naik else F.naive_links(dims, 0.3, 14)
+    m.update_links_milc(np.ascontiguousarray(np.moveaxis(g2[0::2] if naik else g2, 0, 1)),
+                        np.ascontiguousarray(np.moveaxis(g2[1::2], 0, 1)) if naik else None)
+    s.update_links(g2)
+    s.D(a, x, 0.07)
+    m.D(b, x, 0.07)
+    assert np.array_equal(a, b)
