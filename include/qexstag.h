@@ -187,6 +187,14 @@ int qexstag_links_recon12(const qexstag_links *g);
      r = a*r + b*x + sum_k [U_k(s) x(s+d_k) - U_k(s-d_k)^dagger x(s-d_k)]. */
 int qexstag_stagD2(qexstag_links *g, int subset, double *r, const double *x, double a,
                    double b, int mem);
+/* stagDN (stagD.nim:451-455, the multi-vector sweep stagDPN 132-189): for
+   i < n, on subset (EVEN or ODD)
+     r[i] = m*x[i] + sum_k [U_k(s) x[i](s+d_k) - U_k(s-d_k)^dagger x[i](s-d_k)],
+   which is stagD2(subset, r[i], x[i], 0, m) for n fields at once: each link
+   is read once per site for up to 8 of them.  r and x hold n pointers to
+   full-lattice fields; the other parity of each r[i] is not changed. */
+int qexstag_stagDN(qexstag_links *g, int subset, int n, double *const *r, const double *const *x, double m,
+                   int mem);
 /* stagD (stagD.nim:459-462): r = a*r + m*x + (sc/2)(2D)x on subset
    (EVEN, ODD or ALL). */
 int qexstag_stagD(qexstag_links *g, int subset, double *r, const double *x, double m,

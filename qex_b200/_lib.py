@@ -112,6 +112,7 @@ SIGNATURES = {
     "qexstag_links_get_milc": (I, [P, P, P]),
     "qexstag_stagD2": (I, [P, I, P, P, D, D, I]),
     "qexstag_stagD": (I, [P, I, P, P, D, D, D, I]),
+    "qexstag_stagDN": (I, [P, I, I, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), D, I]),
     "qexstag_D": (I, [P, P, P, D, I]),
     "qexstag_Ddag": (I, [P, P, P, D, I]),
     "qexstag_stagD2ee": (I, [P, P, P, D, I]),

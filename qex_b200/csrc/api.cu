@@ -523,6 +523,38 @@ int qexstag_stagD2(qexstag_links *g, int subset, double *r, const double *x, dou
   return stage_out_finish(g, dr, r, mem);
 }
 
+int qexstag_stagDN(qexstag_links *g, int subset, int n, double *const *r, const double *const *x, double m,
+                   int mem) {
+  int rc;
+  if ((rc = check_links(g)) || (rc = check_mem(mem))) return rc;
+  if (n < 1 || !r || !x) return fail(QEXSTAG_ERR_ARG, "stagDN: n must be >= 1 with r and x given");
+  for (int i = 0; i < n; i++)
+    if (!r[i] || !x[i]) return fail(QEXSTAG_ERR_ARG, "stagDN: null field");
+  if (subset != QEXSTAG_EVEN && subset != QEXSTAG_ODD)
+    return fail(QEXSTAG_ERR_ARG, "stagDN: subset must be EVEN or ODD");
+  const Geom &geo = g->l->g;
+  if (mem == QEXSTAG_MEM_DEVICE)
+    return dslashN64(g, subset, n, (double2 *const *)r, geo.V, (const double2 *const *)x, geo.V, m);
+  // host fields: 8 at a time through the staging slots; r is staged in whole
+  // so that its other parity comes back unchanged
+  for (int i0 = 0; i0 < n; i0 += 8) {
+    const int nb = std::min(8, n - i0);
+    const double2 *dx[8];
+    double2 *dr[8];
+    for (int j = 0; j < nb; j++) {
+      const double2 *t;
+      if ((rc = stage_in(g, kSlotDn0 + j, x[i0 + j], mem, &dx[j])) ||
+          (rc = stage_in(g, kSlotDn0 + 8 + j, r[i0 + j], mem, &t)))
+        return rc;
+      dr[j] = const_cast<double2 *>(t);
+    }
+    if ((rc = dslashN64(g, subset, nb, dr, geo.V, dx, geo.V, m))) return rc;
+    for (int j = 0; j < nb; j++)
+      if ((rc = stage_out_finish(g, dr[j], r[i0 + j], mem))) return rc;
+  }
+  return QEXSTAG_OK;
+}
+
 static int stagD_api(qexstag_links *g, int subset, double *r, const double *x, double m, double sc,
                      double a, int mem) {
   int rc;

@@ -37,6 +37,7 @@ enum Slot {
   kSlotFull0, kSlotFull1, kSlotFull2,
   kSlotMx0 = 40,  // mixed-precision vectors and multishift (up to 80 slots)
   kSlotMs0 = 120,
+  kSlotDn0 = 300,  // stagDN host staging: 8 inputs, then 8 outputs
   kSlotLast = 400
 };
 
@@ -77,6 +78,9 @@ enum RedKind { kRedNone = 0, kRedCgPAp = 1, kRedDot = 2 };
 int dslash64(const qexstag_links_s *g, int po, VecD out, CVecD xin, CVecD xs, CVecD rin,
              double a, double b, double c, int hop, int init, int red = kRedNone,
              void *state = nullptr, const int *done = nullptr, double *dot_out = nullptr);
+// stagDN (mrhs.cu): r[i] (parity po) = m x[i] + (2D) x[i], i < n
+int dslashN64(const qexstag_links_s *gl, int po, int n, double2 *const *r, int rstride, const double2 *const *x,
+              int xstride, double m);
 // Schur operator on parity par: r = 4 m2 x - (2D)_{par,q} (2D)_{q,par} x,
 // with t (q block) the temporary; red kRedCgPAp/kRedDot accumulate Re<x, r>.
 int schur64(const qexstag_links_s *g, int par, VecD r, CVecD x, VecD t, double m2,

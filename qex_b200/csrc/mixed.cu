@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "lib.cuh"
 #include "lowprec.cuh"
@@ -655,6 +656,53 @@ int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void
     rc = g->nl == 8 ? sloppy_half<kF16, 8>(1, A, grid, red, red_blocks)
                     : sloppy_half<kF16, 4>(1, A, grid, red, red_blocks);
   return rc;
+}
+
+// sloppy Schur with FP32 vectors whatever the link precision (the
+// single-right-hand-side multi-shift CG): ap = 4 m2 p - (2D)(2D) p on parity
+// par, t the FP32 temporary, *dot_out = Re <p, ap> (FP64 sum)
+int schur_lo_v32(const qexstag_links_s *g, int prec, int par, float2 *ap, const float2 *p, float2 *t, double m2,
+                 double *dot_out) {
+  const Geom &geo = g->l->g;
+  DslashArgsLo A;
+  A.g = geo;
+  A.L = lo_links(g->low, prec);
+  A.halt = nullptr;
+  A.state = nullptr;
+  A.partials = red_partials();
+  A.ticket = red_tickets();
+  A.dot_out = dot_out;
+  A.po = 1 - par;
+  A.xin = p;
+  A.istride = geo.nh;
+  A.xs = nullptr;
+  A.sstride = 0;
+  A.out = t;
+  A.ostride = geo.nh;
+  A.b = 0.f;
+  auto sweeps = [&](auto nl) {
+    constexpr int NL = decltype(nl)::value;
+    if (prec == kF16)
+      launch_lo<kF16, kF32, NL, 1, 0, 0, kF32>(A, 0);
+    else
+      launch_lo<kF32, kF32, NL, 1, 0, 0, kF32>(A, 0);
+    A.po = par;
+    A.xin = t;
+    A.xs = p;
+    A.sstride = geo.nh;
+    A.out = ap;
+    A.b = (float)(4.0 * m2);
+    if (prec == kF16)
+      launch_lo<kF16, kF32, NL, -1, 1, 2, kF32>(A, 0);
+    else
+      launch_lo<kF32, kF32, NL, -1, 1, 2, kF32>(A, 0);
+  };
+  if (g->nl == 8)
+    sweeps(std::integral_constant<int, 8>());
+  else
+    sweeps(std::integral_constant<int, 4>());
+  QS_LAUNCH_CHECK();
+  return QEXSTAG_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -467,14 +467,20 @@ static int read_cgm_head(const CgmState *d, CgmState *h) {
 }
 
 int check_interval(int nh);
+int schur_lo_v32(const qexstag_links_s *g, int prec, int par, float2 *ap, const float2 *p, float2 *t, double m2,
+                 double *dot_out);
+int cg_mixed(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2req, int maxits, int sloppy,
+             double delta, CgOut *out, int *reliable);
 
 // Multi-shift CG on parity par: (A + sg[k]) x_jk = b_j, A = stagD2xx(m2),
-// sg[0] = 0.  fp32: FP32 vectors with the multi-rhs FP32 Dslash, else FP64
-// (nrhs must be 1).  Solutions are written to y[j*nshift+k] (FP64 blocks of
-// parity par with stride ystride) scaled by yscale.
+// sg[0] = 0.  fp32: FP32 vectors with the multi-rhs FP32 Dslash (one
+// right-hand side: the single-vector sloppy Schur with links of precision
+// lprec, kF32 or kF16), else FP64 (nrhs must be 1).  Solutions are written
+// to y[j*nshift+k] (FP64 blocks of parity par with stride ystride) scaled by
+// yscale.
 static int cgm_core(qexstag_links_s *g, int par, double m2, int nshift, const double *sg, int nrhs,
                     const double2 *const *b, int bstride, double2 *const *y, int ystride, double yscale,
-                    double r2req, int maxits, bool fp32, bool dropping, int *iters) {
+                    double r2req, int maxits, bool fp32, bool dropping, int *iters, int lprec = kF32) {
   const Geom &geo = g->l->g;
   const int nh = geo.nh;
   Workspace &ws = g->ws;
@@ -516,7 +522,11 @@ static int cgm_core(qexstag_links_s *g, int par, double m2, int nshift, const do
     for (;;) {
       for (int i = 0; i < every; i++) {
         // p_0 of right-hand side j lives at xs_off(j, 0)
-        if ((rc = schur_mrhs(g, par, nrhs, v.p, v.xs_off(1, 0), v.t, v.ap, m2, st))) return rc;
+        if (nrhs == 1)
+          rc = schur_lo_v32(g, lprec, par, v.ap, v.p, v.t, m2, &st->pAp[0]);
+        else
+          rc = schur_mrhs(g, par, nrhs, v.p, v.xs_off(1, 0), v.t, v.ap, m2, st);
+        if (rc) return rc;
         cgm_alpha_kernel<<<1, 1, 0, stream()>>>(st);
         cgm_update1_kernel<float2><<<grid, kBlock, 0, stream()>>>(v, st, red_partials(), red_tickets());
         cgm_update2_kernel<float2><<<egrid, kBlock, 0, stream()>>>(v, st);
@@ -688,7 +698,8 @@ int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nr
     }
     int its = 0;
     if (sloppy) {
-      rc = cgm_core(g, 0, m2, nshift, sg.data(), nr, bb, V, yy, V, 1.0, r2ms, maxits, true, true, &its);
+      rc = cgm_core(g, 0, m2, nshift, sg.data(), nr, bb, V, yy, V, 1.0, r2ms, maxits, true, true, &its,
+                    p->sloppy == QEXSTAG_SLOPPY_HALF ? kF16 : kF32);
     } else {
       rc = 0;
       for (int j = 0; j < nr && !rc; j++) {
@@ -753,9 +764,20 @@ int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nr
             dy[q] = dbuf[live[q]];
           }
           int its = 0;
-          if ((rc = cgm_core(g, 0, m2s, 1, &zero, (int)live.size(), rb, nh, dy, nh, 1.0, req,
-                             maxits - st->iterations, true, false, &its)))
+          if (live.size() == 1) {
+            // one system: the reliable-update CG in the call's sloppy precision
+            CgOut o{};
+            int rel = 0;
+            const double delta = p->delta > 0 ? p->delta : 0.1;
+            if ((rc = cg_mixed(g, 0, m2s, CVecD{rb[0], nh}, VecD{dy[0], nh}, req, maxits - st->iterations,
+                               p->sloppy, delta, &o, &rel)))
+              return rc;
+            its = o.iterations;
+            st->reliable_updates += rel;
+          } else if ((rc = cgm_core(g, 0, m2s, 1, &zero, (int)live.size(), rb, nh, dy, nh, 1.0, req,
+                                    maxits - st->iterations, true, false, &its))) {
             return rc;
+          }
           st->iterations += its;
           st->outer_iterations += 1;
           for (size_t q = 0; q < live.size(); q++) {

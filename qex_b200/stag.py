@@ -256,6 +256,18 @@ class Staggered:
         L.check(self._lib.qexstag_stagD2(self.handle, subset, _ptr(r, True)[0], _ptr(x)[0],
                                          float(a), float(b), mem), "stagD2")
 
+    def stagDN(self, subset: int, rs, xs, m: float) -> None:
+        """stagDN (stagD.nim:451-455): rs[i] = m xs[i] + (2D) xs[i] on the
+        subset for every i, each link read once per site for up to 8
+        fields."""
+        if len(rs) != len(xs) or not rs:
+            raise ValueError("stagDN needs equally many (>= 1) outputs and inputs")
+        mem = _mem_of(*rs, *xs)
+        n = len(rs)
+        ra = (C.c_void_p * n)(*[_ptr(r, True)[0] for r in rs])
+        xa = (C.c_void_p * n)(*[_ptr(x)[0] for x in xs])
+        L.check(self._lib.qexstag_stagDN(self.handle, subset, n, ra, xa, float(m), mem), "stagDN")
+
     def stagD(self, subset: int, r, x, m: float, sc: float = 1.0, a: float = 0.0) -> None:
         mem = _mem_of(r, x)
         L.check(self._lib.qexstag_stagD(self.handle, subset, _ptr(r, True)[0], _ptr(x)[0],

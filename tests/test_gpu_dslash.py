@@ -211,3 +211,35 @@ def test_links_milc_order(cuda, naik):
     s.D(a, x, 0.07)
     m.D(b, x, 0.07)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("naik", [False, True])
+@pytest.mark.parametrize("n", [1, 3, 11])
+def test_stagDN_matches_oracle(cuda, naik, n):
+    """stagDN (stagD.nim:451-455): r_i = m x_i + (2D) x_i on one subset for
+    n fields at once equals the oracle's stagD2(subset, r_i, x_i, 0, m) for
+    every i, host and device paths; the other parity of r_i is unchanged.
+    n = 11 spans two launches of the 8-field kernel."""
+    torch = cuda
+    dims = (8, 4, 6, 8)
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 17) if naik else F.naive_links(dims, 0.3, 17)
+    o = O.Oracle(dims, g)
+    s = S.Staggered(S.Layout(dims), g)
+    m = 0.37
+    xs = [F.gaussian_vector(V, 100 + i) for i in range(n)]
+    for subset in (L.EVEN, L.ODD):
+        other = slice(V // 2, V) if subset == L.EVEN else slice(0, V // 2)
+        mine = slice(0, V // 2) if subset == L.EVEN else slice(V // 2, V)
+        rs = [np.full((V, 3), 3.0 + 1j) for _ in range(n)]
+        s.stagDN(subset, rs, xs, m)
+        rd = [torch.full((3, V), 2.0 - 1j, dtype=torch.complex128, device="cuda") for _ in range(n)]
+        s.stagDN(subset, rd, [S.to_device_vector(x) for x in xs], m)
+        for i in range(n):
+            ro = o.vec()
+            o.stagD2(subset, ro, xs[i], 0.0, m)
+            assert rel(rs[i][mine], ro[mine]) < TOL, (subset, i)
+            assert np.all(rs[i][other] == 3.0 + 1j)
+            rh = S.to_host_vector(rd[i])
+            assert np.array_equal(rh[mine], rs[i][mine])
+            assert np.all(rh[other] == 2.0 - 1j)
