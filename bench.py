@@ -240,6 +240,80 @@ def timed_solves(s, yd, bd, sp_kw, steps, torch):
     return times, launches, iters, sps
 
 
+def time_multishift(s, dims, torch):
+    """The mixed-precision multi-shift solve on the workload's lattice and
+    fields: one Gaussian right-hand side, 12 shifts log-spaced from 1e-4 to
+    1 (A + sigma_k, A = stagD2ee(m^2)), true FP64 residual 1e-10 for every
+    shift; 16-bit links in the multi-shift iterations, then each shift
+    refined by the reliable-update CG.  Beside it, the same systems by FP64
+    multi-shift CG and by one plain FP64 CG per shift.  One warm-up and one
+    timed call each (CUDA events)."""
+    from qex_b200 import fields as F
+    from qex_b200 import stag as S
+    from qex_b200.multishift_bench import shifts
+    V = F.volume(dims)
+    sig = shifts(12)
+    b = S.to_device_vector(F.even_source(dims, 100))
+    ys = [torch.zeros((3, V), dtype=torch.complex128, device="cuda") for _ in sig]
+
+    def timed(fn, reps):
+        for i in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = fn()
+            e1.record()
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3, out
+
+    res = {}
+    for name, sl in (("mixed_16bit", 2), ("fp64_multishift", 0)):
+        sp = S.SolverParams(r2req=R2REQ, sloppySolve=sl, delta=DELTA)
+        t, r2 = timed(lambda: s.cgm_ee(MASS, sig, [b], [ys], sp), 2)
+        res[name] = {"time_s": t, "iterations": sp.iterations, "max_true_r2": float(r2.max())}
+
+    def separate():
+        its, worst = 0, 0.0
+        for k, sg in enumerate(sig):
+            sp = S.SolverParams(r2req=R2REQ)
+            s.solveEE(ys[k], b, float(np.sqrt(MASS * MASS + 0.25 * sg)), sp)
+            its += sp.iterations
+            worst = max(worst, sp.r2)
+        return its, worst
+
+    t, (its, worst) = timed(separate, 1)
+    res["fp64_cg_per_shift"] = {"time_s": t, "iterations": its, "max_true_r2": worst}
+    m = res["mixed_16bit"]["time_s"]
+    return {"workload": f"{'x'.join(map(str, dims))}, m={MASS}, 1 Gaussian right-hand side, 12 shifts "
+                        "10^-4..1, true r2 <= 1e-20 per shift", "solvers": res,
+            "speedup_vs_fp64_cg_per_shift": res["fp64_cg_per_shift"]["time_s"] / m,
+            "speedup_vs_fp64_multishift": res["fp64_multishift"]["time_s"] / m}
+
+
+def time_stagdn(s, nh, torch, peak):
+    """stagDN (FP64 multi-field Dslash) on 1 and 8 fields: device time per
+    call and HBM throughput against its compulsory bytes per output site,
+    links 16 x 144 B + fields x (48 B own site + 48 B neighbours + 48 B out)."""
+    out = {}
+    V = 2 * nh
+    xs = [torch.randn((3, V), dtype=torch.complex128, device="cuda") for _ in range(8)]
+    rs = [torch.zeros_like(x) for x in xs]
+    for n in (1, 8):
+        for rep in range(2):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                s.stagDN(0, rs[:n], xs[:n], 0.1)
+            e1.record()
+            torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3 / 10
+        byt = (16 * 144 + n * 144) * nh
+        out[f"fields_{n}"] = {"us": round(t * 1e6, 1), "GBps": round(byt / t / 1e9, 1),
+                              "frac": round(byt / t / 1e9 / peak, 4), "bytes_per_site": 16 * 144 + n * 144}
+    return out
+
+
 def run_ours(args, dims):
     import torch
 
@@ -328,6 +402,9 @@ def run_ours(args, dims):
         e2e_times.append(time.perf_counter() - t0)
     e2e = max_over_ranks(float(np.mean(e2e_times)), ws)
 
+    multishift = None if args.no_multishift else time_multishift(s, dims, torch)
+    stagdn = time_stagdn(s, nh, torch, peak)
+
     line = None
     if rank == 0:
         cpu = None
@@ -350,6 +427,7 @@ def run_ours(args, dims):
                 "fp64_time_s": results["fp64"]["time_s"],
                 "speedup_vs_fp64": results["fp64"]["time_s"] / value,
                 "roofline": roof, "cpu_baseline": cpu,
+                "multishift": multishift, "multi_rhs_dslash": stagdn,
                 "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(bh.nbytes) // 2,
                         "d2h_bytes_per_step": int(yh.nbytes), "host_memory": "pinned"},
                 "clocks": results[best]["clocks"],
@@ -374,6 +452,7 @@ def main():
     ap.add_argument("--ref-warm-iters", type=int, default=5)
     ap.add_argument("--ref-maxits", type=int, default=100000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-multishift", action="store_true", help="skip the multi-shift comparison")
     args = ap.parse_args()
     dims = tuple(int(v) for v in args.dims.split(","))
     if args.impl == "reference":

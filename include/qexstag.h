@@ -499,6 +499,30 @@ int qexstag_domain_connect_local(qexstag_domain *const *doms, int n);
    with qexstag_nccl_unique_id and every rank received. */
 int qexstag_nccl_unique_id(void *id128);
 int qexstag_domain_connect_nccl(qexstag_domain *d, const void *id128);
+/* A communicator supplied by the host, for one domain per process without
+   NCCL: the shape of QEX's Comm object (src/comms/comms.nim:6-28: pushSend,
+   pushRecv, waitSends/waitRecvs, allReduce over float64), e.g. MPI, QMP or
+   a test harness.  For each exchange the library stages the boundary faces
+   in host memory, posts both receives and both sends, then calls wait_all;
+   buffers stay valid until wait_all returns.  A message goes to rank `rank`
+   with tag 0 (travelling up in t: my top slices to the up neighbour's lower
+   ghosts), 1 (down in t), 2 (up in z) or 3 (down in z); the receiver posts
+   the same tag, and messages with one tag between one pair of ranks are
+   matched in the order they are posted.  all_reduce_sum replaces x[0..n) by
+   its sum over all ranks, the same value on every rank.  Each callback
+   returns 0 on success; any other value makes the library call fail with
+   QEXSTAG_ERR_STATE. */
+typedef struct {
+  void *ctx;
+  int (*push_send)(void *ctx, int rank, int tag, const void *buf, size_t bytes);
+  int (*push_recv)(void *ctx, int rank, int tag, void *buf, size_t bytes);
+  int (*wait_all)(void *ctx);
+  int (*all_reduce_sum)(void *ctx, double *x, int n);
+} qexstag_host_comm;
+/* One domain per process, connected through comm (copied; comm->ctx must
+   stay valid while the domain is in use).  Every process makes the same
+   calls in the same order, as for NCCL. */
+int qexstag_domain_connect_host(qexstag_domain *d, const qexstag_host_comm *comm);
 /* Set each domain's links (links[k] for doms[k]) and exchange their
    boundary slices. */
 int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const *links, int mem);

@@ -158,6 +158,7 @@ SIGNATURES = {
     "qexstag_domain_connect_local": (I, [PP, I]),
     "qexstag_nccl_unique_id": (I, [P]),
     "qexstag_domain_connect_nccl": (I, [P, P]),
+    "qexstag_domain_connect_host": (I, [P, P]),
     "qexstag_domain_links": (I, [PP, I, PP, I]),
     "qexstag_domain_stagD2ee": (I, [PP, I, PP, PP, D, I]),
     "qexstag_domain_solveEE": (I, [PP, I, PP, PP, D, P, P, I]),

@@ -117,6 +117,10 @@ struct qexstag_domain_s {
   qexstag_domain_s *up = nullptr, *down = nullptr;    // in-process t neighbours
   qexstag_domain_s *zup = nullptr, *zdown = nullptr;  // in-process z neighbours
   ncclComm_t comm = nullptr;        // inter-process neighbours
+  bool hostc = false;               // inter-process through the host communicator hc
+  qexstag_host_comm hc{};
+  void *hbuf = nullptr;             // pinned staging of host-communicator exchanges
+  size_t hbuf_bytes = 0;
   bool connected = false;
   std::vector<qs::Geom> local;      // geometry of the T-slice local lattice
   double *dsum = nullptr;           // device scalars: see DevScalars
@@ -172,6 +176,41 @@ static int find_in_set(qexstag_domain_s *const *ds, int n, const qexstag_domain_
   return -1;
 }
 
+// pinned staging for the host communicator: four buffers of bytes each
+// (send down, send up, receive down, receive up)
+static int host_bufs(qexstag_domain_s *d, size_t bytes, char **b) {
+  if (d->hbuf_bytes < 4 * bytes) {
+    if (d->hbuf) {
+      cudaStreamSynchronize(stream());
+      cudaStreamSynchronize(d->side);
+      cudaFreeHost(d->hbuf);
+      d->hbuf = nullptr;
+      d->hbuf_bytes = 0;
+    }
+    if (cudaHostAlloc(&d->hbuf, 4 * bytes, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      d->hbuf = nullptr;
+      return fail(QEXSTAG_ERR_ALLOC, "domain: pinned staging for the host communicator failed");
+    }
+    d->hbuf_bytes = 4 * bytes;
+  }
+  *b = (char *)d->hbuf;
+  return QEXSTAG_OK;
+}
+
+// One exchange through the host communicator: receive both ghost faces,
+// send both boundary faces (tag: direction of travel), wait.  The faces are
+// in host memory already (sdn, sup), the received ones land in rdn, rup.
+static int host_swap(qexstag_domain_s *d, int dnr, int upr, const void *sdn, const void *sup, void *rdn, void *rup,
+                     size_t bytes, int tag_up, int tag_dn) {
+  const qexstag_host_comm &c = d->hc;
+  if (c.push_recv(c.ctx, dnr, tag_up, rdn, bytes) || c.push_recv(c.ctx, upr, tag_dn, rup, bytes) ||
+      c.push_send(c.ctx, upr, tag_up, sup, bytes) || c.push_send(c.ctx, dnr, tag_dn, sdn, bytes) ||
+      c.wait_all(c.ctx))
+    return fail(QEXSTAG_ERR_STATE, "domain: the host communicator reported an error");
+  return QEXSTAG_OK;
+}
+
 // z ghost rows of every t slice of one parity block (after the t ghosts)
 static int exchange_z(qexstag_domain_s *const *ds, int n, double2 *const *base, int ncomp, int par,
                       cudaStream_t s) {
@@ -181,7 +220,33 @@ static int exchange_z(qexstag_domain_s *const *ds, int n, double2 *const *base, 
   for (int k = 0; k < n; k++) {
     qexstag_domain_s *d = ds[k];
     const size_t V = (size_t)d->ext->g.V, off = (size_t)par * d->ext->g.nh;
-    if (d->comm) {
+    if (d->hostc) {
+      const int upr = rank_of(d, d->rz + 1, d->rt), dnr = rank_of(d, d->rz - 1, d->rt);
+      for (int c0 = 0; c0 < ncomp; c0 += 3) {
+        const int nc = std::min(3, ncomp - c0);
+        const size_t face = (size_t)nc * rows * width, bytes = face * sizeof(double2);
+        void *pb;
+        char *hb;
+        int rc = d->g->ws.get(kDmPack, sizeof(double2) * 4 * (size_t)3 * rows * width, &pb);
+        if (rc || (rc = host_bufs(d, bytes, &hb))) return rc;
+        double2 *sdn = (double2 *)pb, *sup = sdn + face, *rdn = sup + face, *rup = rdn + face;
+        double2 *f = base[k] + (size_t)c0 * V;
+        const int grid = grid_for((long)face);
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off + (size_t)hz * P, pitch, sdn, nc, rows, width, 1);
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off + (size_t)Z * P, pitch, sup, nc, rows, width, 1);
+        note_launch(2);
+        QS_LAUNCH_CHECK();
+        QS_CUDA(cudaMemcpyAsync(hb, sdn, 2 * bytes, cudaMemcpyDeviceToHost, s));  // sdn, sup are adjacent
+        QS_CUDA(cudaStreamSynchronize(s));
+        if ((rc = host_swap(d, dnr, upr, hb, hb + bytes, hb + 2 * bytes, hb + 3 * bytes, bytes, 2, 3))) return rc;
+        QS_CUDA(cudaMemcpyAsync(rdn, hb + 2 * bytes, 2 * bytes, cudaMemcpyHostToDevice, s));  // rdn, rup adjacent
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off, pitch, rdn, nc, rows, width, 0);
+        face_copy_kernel<<<grid, kBlock, 0, s>>>(f, V, off + (size_t)(hz + Z) * P, pitch, rup, nc, rows, width, 0);
+        note_launch(2);
+        QS_LAUNCH_CHECK();
+        QS_CUDA(cudaStreamSynchronize(s));
+      }
+    } else if (d->comm) {
       const int upr = rank_of(d, d->rz + 1, d->rt), dnr = rank_of(d, d->rz - 1, d->rt);
       for (int c0 = 0; c0 < ncomp; c0 += 3) {
         const int nc = std::min(3, ncomp - c0);
@@ -237,7 +302,29 @@ static int exchange(qexstag_domain_s *const *ds, int n, double2 *const *base, in
     qexstag_domain_s *d = ds[k];
     const size_t V = (size_t)d->ext->g.V, nh = (size_t)d->ext->g.nh;
     const size_t cnt = d->h * sh;  // sites per face per component
-    if (d->comm) {
+    if (d->hostc) {
+      // faces of every component through pinned host memory, [ncomp][cnt]
+      const int upr = rank_of(d, d->rz, d->rt + 1), dnr = rank_of(d, d->rz, d->rt - 1);
+      const size_t per = cnt * sizeof(double2), bytes = per * ncomp;
+      char *hb;
+      int rc = host_bufs(d, bytes, &hb);
+      if (rc) return rc;
+      char *sdn = hb, *sup = hb + bytes, *rdn = hb + 2 * bytes, *rup = hb + 3 * bytes;
+      for (int c = 0; c < ncomp; c++) {
+        const double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
+        QS_CUDA(cudaMemcpyAsync(sup + c * per, f + (size_t)d->T * sh, per, cudaMemcpyDeviceToHost, s));
+        QS_CUDA(cudaMemcpyAsync(sdn + c * per, f + (size_t)d->h * sh, per, cudaMemcpyDeviceToHost, s));
+      }
+      QS_CUDA(cudaStreamSynchronize(s));
+      if ((rc = host_swap(d, dnr, upr, sdn, sup, rdn, rup, bytes, 0, 1))) return rc;
+      for (int c = 0; c < ncomp; c++) {
+        double2 *f = base[k] + (size_t)c * V + (size_t)par * nh;
+        QS_CUDA(cudaMemcpyAsync(f, rdn + c * per, per, cudaMemcpyHostToDevice, s));
+        QS_CUDA(cudaMemcpyAsync(f + (size_t)(d->h + d->T) * sh, rup + c * per, per, cudaMemcpyHostToDevice, s));
+      }
+      // the staging is reused by the next exchange: let these copies finish
+      QS_CUDA(cudaStreamSynchronize(s));
+    } else if (d->comm) {
       QS_NCCL(nccl().groupStart());
       const int upr = rank_of(d, d->rz, d->rt + 1), dnr = rank_of(d, d->rz, d->rt - 1);
       for (int c = 0; c < ncomp; c++) {
@@ -272,7 +359,10 @@ static int allreduce_sum(qexstag_domain_s *const *ds, int n, const double *vals,
   double s = 0;
   for (int k = 0; k < n; k++) s += vals[k];
   qexstag_domain_s *d = ds[0];
-  if (d->comm) {
+  if (d->hostc) {
+    if (d->hc.all_reduce_sum(d->hc.ctx, &s, 1))
+      return fail(QEXSTAG_ERR_STATE, "domain: the host communicator's sum reported an error");
+  } else if (d->comm) {
     QS_CUDA(cudaMemcpyAsync(d->dsum, &s, sizeof(double), cudaMemcpyHostToDevice, stream()));
     QS_NCCL(nccl().allReduce(d->dsum, d->dsum, 1, ncclDouble, ncclSum, d->comm, stream()));
     QS_CUDA(cudaMemcpyAsync(&s, d->dsum, sizeof(double), cudaMemcpyDeviceToHost, stream()));
@@ -329,11 +419,12 @@ static int check_set(qexstag_domain_s *const *ds, int n) {
     if (ds[k]->nl != ds[0]->nl || std::memcmp(ds[k]->gdims, ds[0]->gdims, sizeof ds[0]->gdims) ||
         ds[k]->nranks != ds[0]->nranks || ds[k]->Rz != ds[0]->Rz || ds[k]->hz != ds[0]->hz)
       return fail(QEXSTAG_ERR_ARG, "domain: domains of different lattices in one call");
-    if ((ds[k]->comm != nullptr) != (ds[0]->comm != nullptr))
-      return fail(QEXSTAG_ERR_ARG, "domain: in-process and NCCL domains in one call");
+    if ((ds[k]->comm != nullptr) != (ds[0]->comm != nullptr) || ds[k]->hostc != ds[0]->hostc)
+      return fail(QEXSTAG_ERR_ARG, "domain: domains with different connections in one call");
   }
   if (n > kMaxSet) return fail(QEXSTAG_ERR_ARG, "domain: more than 64 domains in one call");
-  if (ds[0]->comm && n > 1) return fail(QEXSTAG_ERR_ARG, "domain: one NCCL-connected domain per call");
+  if ((ds[0]->comm || ds[0]->hostc) && n > 1)
+    return fail(QEXSTAG_ERR_ARG, "domain: one NCCL- or host-connected domain per call");
   return runtime_ready();
 }
 
@@ -563,7 +654,24 @@ __global__ void dm_scalar_kernel(const double *slots, int n, double *val, CgStat
 
 static int finish_scalar(qexstag_domain_s *const *ds, int n, CgState *st, int what) {
   double *slots = ds[0]->dsum, *val = ds[0]->dsum + kValOff;
-  if (ds[0]->comm) {
+  if (ds[0]->hostc) {
+    // through the host: this process's value out, the sum over processes in
+    double *h = host_results();
+    dm_scalar_kernel<<<1, 1, 0, stream()>>>(slots, n, val, st, 0);
+    note_launch();
+    QS_LAUNCH_CHECK();
+    QS_CUDA(cudaMemcpyAsync(h, val, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+    QS_CUDA(cudaStreamSynchronize(stream()));
+    double v = h[0];
+    if (ds[0]->hc.all_reduce_sum(ds[0]->hc.ctx, &v, 1))
+      return fail(QEXSTAG_ERR_STATE, "domain: the host communicator's sum reported an error");
+    h[0] = v;
+    QS_CUDA(cudaMemcpyAsync(val, h, sizeof(double), cudaMemcpyHostToDevice, stream()));
+    dm_scalar_kernel<<<1, 1, 0, stream()>>>(nullptr, 0, val, st, what);
+    note_launch();
+    // h is reused by the next call: the copy must have read it
+    QS_CUDA(cudaStreamSynchronize(stream()));
+  } else if (ds[0]->comm) {
     dm_scalar_kernel<<<1, 1, 0, stream()>>>(slots, n, val, st, 0);
     QS_NCCL(nccl().allReduce(val, val, 1, ncclDouble, ncclSum, ds[0]->comm, stream()));
     dm_scalar_kernel<<<1, 1, 0, stream()>>>(nullptr, 0, val, st, what);
@@ -733,6 +841,11 @@ int qexstag_domain_create_zt(const int global_dims[4], const int grid[2], int ra
 int qexstag_domain_destroy(qexstag_domain *d) {
   if (!d) return QEXSTAG_OK;
   if (d->comm && nccl().ok) nccl().commDestroy(d->comm);
+  if (d->hbuf) {
+    cudaStreamSynchronize(stream());
+    if (d->side) cudaStreamSynchronize(d->side);
+    cudaFreeHost(d->hbuf);
+  }
   if (d->g) qexstag_links_destroy(d->g);
   if (d->ext) qexstag_layout_destroy(d->ext);
   if (d->dsum) cudaFree(d->dsum);
@@ -785,9 +898,20 @@ int qexstag_nccl_unique_id(void *id) {
 int qexstag_domain_connect_nccl(qexstag_domain *d, const void *id) {
   if (!d || !id) return fail(QEXSTAG_ERR_ARG, "domain_connect_nccl: null argument");
   if (!nccl().ok) return fail(QEXSTAG_ERR_STATE, "domain_connect_nccl: libnccl.so.2 not available");
+  if (d->connected) return fail(QEXSTAG_ERR_STATE, "domain_connect_nccl: the domain is already connected");
   ncclUniqueId u;
   std::memcpy(&u, id, sizeof u);
   QS_NCCL(nccl().commInitRank(&d->comm, d->nranks, u, d->rank));
+  d->connected = true;
+  return QEXSTAG_OK;
+}
+
+int qexstag_domain_connect_host(qexstag_domain *d, const qexstag_host_comm *comm) {
+  if (!d || !comm || !comm->push_send || !comm->push_recv || !comm->wait_all || !comm->all_reduce_sum)
+    return fail(QEXSTAG_ERR_ARG, "domain_connect_host: null domain, communicator or callback");
+  if (d->connected) return fail(QEXSTAG_ERR_STATE, "domain_connect_host: the domain is already connected");
+  d->hc = *comm;
+  d->hostc = true;
   d->connected = true;
   return QEXSTAG_OK;
 }

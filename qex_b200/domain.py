@@ -1,8 +1,9 @@
 """Domain decomposition along t through the C ABI (qexstag_domain_*): QEX's
 rank split of the lattice (rankGeom; src/layout/shifts.nim, qshifts.nim)
 with ghost-slice exchanges.  A process holds either every rank's domain
-(one device, exchanges by device copies) or one (one rank per GPU,
-exchanges and sums by NCCL).
+(one device, exchanges by device copies) or one (one rank per process,
+exchanges and sums by NCCL, or through a host communicator such as
+TorchHostComm over a torch.distributed process group).
 
 Global host fields are split into rank slabs here for convenience: links
 (nlinks, V, 3, 3) and colour vectors (V, 3) in the global V=1 order.
@@ -22,6 +23,85 @@ def _arr(ptrs):
     return (C.c_void_p * len(ptrs))(*ptrs)
 
 
+_PUSH = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t)
+_WAIT = C.CFUNCTYPE(C.c_int, C.c_void_p)
+_SUM = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_int)
+
+
+class HostCommC(C.Structure):
+    """qexstag_host_comm"""
+    _fields_ = [("ctx", C.c_void_p), ("push_send", _PUSH), ("push_recv", _PUSH), ("wait_all", _WAIT),
+                ("all_reduce_sum", _SUM)]
+
+
+class TorchHostComm:
+    """qexstag_host_comm over a torch.distributed process group (gloo, or
+    any backend that sends CPU tensors): the shape of QEX's Comm object
+    (src/comms/comms.nim: pushSend, pushRecv, waitSends/waitRecvs,
+    allReduce).  Messages to this process's own rank (a grid with one rank
+    along a direction) are copied in memory.  Callbacks return 1 on any
+    exception, which the library reports as an error."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.me = dist.get_rank(group)
+        self.reqs = []
+        self.self_recv = []  # (tag, address, bytes) posted to this rank itself
+        self._cbs = (_PUSH(self._send), _PUSH(self._recv), _WAIT(self._wait), _SUM(self._sum))
+        self.struct = HostCommC(None, *self._cbs)
+
+    @staticmethod
+    def _view(addr, nbytes):
+        import torch
+        return torch.from_numpy(np.ctypeslib.as_array((C.c_uint8 * nbytes).from_address(addr)))
+
+    def _send(self, ctx, rank, tag, buf, nbytes):
+        try:
+            if rank == self.me:
+                for i, (t, a, n) in enumerate(self.self_recv):
+                    if t == tag and n == nbytes:
+                        C.memmove(a, buf, nbytes)
+                        del self.self_recv[i]
+                        return 0
+                return 1
+            t = self._view(buf, nbytes)
+            self.reqs.append((self.dist.isend(t, dst=rank, group=self.group, tag=tag), t))
+            return 0
+        except Exception:
+            return 1
+
+    def _recv(self, ctx, rank, tag, buf, nbytes):
+        try:
+            if rank == self.me:
+                self.self_recv.append((tag, buf, nbytes))
+                return 0
+            t = self._view(buf, nbytes)
+            self.reqs.append((self.dist.irecv(t, src=rank, group=self.group, tag=tag), t))
+            return 0
+        except Exception:
+            return 1
+
+    def _wait(self, ctx):
+        try:
+            for r, _ in self.reqs:
+                r.wait()
+            self.reqs.clear()
+            return 0 if not self.self_recv else 1
+        except Exception:
+            return 1
+
+    def _sum(self, ctx, x, n):
+        try:
+            import torch
+            t = torch.from_numpy(np.ctypeslib.as_array(x, shape=(n,)))
+            self.dist.all_reduce(t, group=self.group)
+            return 0
+        except Exception:
+            return 1
+
+
 def rank_sites(global_dims, local_dims, grid, rank: int) -> np.ndarray:
     """Global V=1 index of each site of rank's local lattice, in the local
     V=1 order: rank = rz + Rz rt holds z rows [rz Z, (rz+1) Z) of slices
@@ -38,8 +118,8 @@ class DomainSet:
     Rz Rt, rank = rz + Rz rt)."""
 
     def __init__(self, global_dims, nranks: int, nlinks: int, ranks=None, nccl_id: bytes | None = None,
-                 grid=None):
-        S.init(0)
+                 grid=None, host_comm: TorchHostComm | None = None, device: int = 0):
+        S.init(device)
         self.lib = L.load()
         self.gdims = tuple(int(d) for d in global_dims)
         self.grid = (1, nranks) if grid is None else (int(grid[0]), int(grid[1]))
@@ -61,7 +141,11 @@ class DomainSet:
         ld = (C.c_int * 4)()
         L.check(self.lib.qexstag_domain_local_dims(self.handles[0], ld), "domain_local_dims")
         self.ldims = tuple(ld)
-        if nccl_id is None:
+        self.host_comm = host_comm  # keeps the callbacks alive
+        if host_comm is not None:
+            for h in self.handles:
+                L.check(self.lib.qexstag_domain_connect_host(h, C.byref(host_comm.struct)), "domain_connect_host")
+        elif nccl_id is None:
             L.check(self.lib.qexstag_domain_connect_local(self._set(), len(self.handles)), "domain_connect_local")
         else:
             buf = C.create_string_buffer(bytes(nccl_id), 128)

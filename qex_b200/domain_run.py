@@ -39,7 +39,7 @@ def main():
     obj = [DD.nccl_unique_id() if rank == 0 else None]
     dist.broadcast_object_list(obj, src=0)
     grid = (a.zranks, world // a.zranks) if a.zranks > 0 else None
-    d = DD.DomainSet(dims, world, 8, ranks=[rank], nccl_id=obj[0], grid=grid)
+    d = DD.DomainSet(dims, world, 8, ranks=[rank], nccl_id=obj[0], grid=grid, device=local)
     g = F.fat_naik_links(dims, 21)
     b = F.even_source(dims, 31)
     d.set_links(g)

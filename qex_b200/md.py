@@ -158,6 +158,62 @@ class MD:
             link_update(self.l, U, P, eps)
             self.mdv(U, P, eps if i < nsteps - 1 else 0.5 * eps)
 
+    def omelyan(self, U, P, tau: float, nsteps: int, lam: float = 0.1931833275037836) -> None:
+        """In place: Omelyan's second-order minimum-norm integrator (Omelyan,
+        Mryglod and Folk, Comput. Phys. Commun. 151 (2003) 272), QEX's
+        default "2MN" (hmcAction.nim:230, from the mdevolve package).  Per
+        step p += lam eps F, U by eps/2, p += (1 - 2 lam) eps F, U by eps/2,
+        p += lam eps F, the closing kick merged with the next step's opening
+        one: two force evaluations per step."""
+        eps = tau / nsteps
+        self.mdv(U, P, lam * eps)
+        for i in range(nsteps):
+            link_update(self.l, U, P, 0.5 * eps)
+            self.mdv(U, P, (1.0 - 2.0 * lam) * eps)
+            link_update(self.l, U, P, 0.5 * eps)
+            self.mdv(U, P, 2.0 * lam * eps if i < nsteps - 1 else lam * eps)
+
+    def integrate(self, U, P, tau: float, nsteps: int, integrator: str = "leapfrog") -> None:
+        if integrator == "leapfrog":
+            self.leapfrog(U, P, tau, nsteps)
+        elif integrator == "omelyan":
+            self.omelyan(U, P, tau, nsteps)
+        else:
+            raise ValueError(f"unknown integrator {integrator!r}")
+
+
+def plaquette(layout, U) -> float:
+    """Average plaquette Re Tr P / 3 from the Wilson action at beta = 3."""
+    return -GaugeAction(layout, 3.0).action(U) / (6.0 * layout.V * 3.0)
+
+
+def hmc(layout, U, beta, fermion, ntraj, tau=1.0, nsteps=20, integrator="omelyan", seed=7, counter0=0,
+        accept_seed=11):
+    """ntraj HMC trajectories from U (QEX's hmc loop: momenta heatbath,
+    pseudofermion heatbath, molecular dynamics, Metropolis accept/reject with
+    probability min(1, exp(-dH))).  Returns the final links and one record
+    per trajectory (dH, accepted, plaquette after)."""
+    import torch
+    md = MD(layout, GaugeAction(layout, beta), fermion)
+    rng = np.random.default_rng(accept_seed)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    P = torch.empty_like(U)
+    out = []
+    for t in range(ntraj):
+        momenta_heatbath(layout, P, seed, counter0 + t)
+        if fermion is not None:
+            fermion.heatbath(U, gen)
+        h0 = md.hamiltonian(U, P)
+        U1 = U.clone()
+        md.integrate(U1, P, tau, nsteps, integrator)
+        dh = md.hamiltonian(U1, P) - h0
+        acc = bool(dh <= 0 or rng.random() < np.exp(-dh))
+        if acc:
+            U = U1
+        out.append({"dH": dh, "accepted": acc, "plaquette": plaquette(layout, U)})
+    return U, out
+
 
 def trajectory_with_reversal(layout, U0, beta, tau, nsteps, fermion=None, seed=7, counter=0, P0=None):
     """One trajectory from (U0, P0) and back with flipped momenta."""
@@ -231,12 +287,39 @@ def main():
     ap.add_argument("--mass", type=float, default=0.05)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--thin", action="store_true")
+    ap.add_argument("--hmc", type=int, default=0,
+                    help="run this many HMC trajectories with accept/reject instead (after --therm)")
+    ap.add_argument("--therm", type=int, default=20, help="pure-gauge trajectories before --hmc")
+    ap.add_argument("--settle", type=int, default=3, help="trajectories with the fermion before measuring")
+    ap.add_argument("--integrator", default="omelyan", choices=["leapfrog", "omelyan"])
     a = ap.parse_args()
     dims = tuple(int(v) for v in a.dims.split(","))
     S.init(0)
     lay = S.Layout(dims)
     U0 = S.to_device_links(F.gauge_warm(dims, 0.3, 41))
     ferm = StaggeredPseudofermion(lay, a.mass, hisq=not a.thin)
+    if a.hmc > 0:
+        t0 = time.perf_counter()
+        U, th = hmc(lay, U0, a.beta, None, a.therm, nsteps=a.steps, integrator=a.integrator, seed=3)
+        U, st = hmc(lay, U, a.beta, ferm, a.settle, nsteps=a.steps, integrator=a.integrator, seed=5,
+                    counter0=10000)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        U, rec = hmc(lay, U, a.beta, ferm, a.hmc, nsteps=a.steps, integrator=a.integrator, seed=9, counter0=20000)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        dh = np.array([r["dH"] for r in rec])
+        ex = np.exp(-dh)
+        print(json.dumps({
+            "dims": dims, "beta": a.beta, "mass": a.mass, "fermion": "thin fat+Naik" if a.thin else "hisq",
+            "integrator": a.integrator, "steps": a.steps, "tau": 1.0,
+            "thermalization": {"pure_gauge": a.therm, "accepted": sum(r["accepted"] for r in th),
+                               "with_fermion": a.settle, "plaquette": th[-1]["plaquette"] if th else None},
+            "trajectories": rec, "acceptance": float(np.mean([r["accepted"] for r in rec])),
+            "mean_abs_dH": float(np.abs(dh).mean()), "mean_exp_minus_dH": float(ex.mean()),
+            "exp_minus_dH_stderr": float(ex.std(ddof=1) / np.sqrt(len(ex))) if len(ex) > 1 else None,
+            "seconds_per_trajectory": (t2 - t1) / a.hmc, "seconds_thermalization": t1 - t0}))
+        return
     gen = torch.Generator(device="cuda")
     gen.manual_seed(7)
     ferm.heatbath(U0, gen)

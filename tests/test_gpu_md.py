@@ -1,6 +1,6 @@
 """GPU parity of the molecular-dynamics kernels (gauge action and force,
 link update, momenta) against the oracle, and of the device-side MD driver
-(qex_b200/md.py) against the torch-glue HMC of qex_b200/hmc.py on the same
+(qex_b200/md.py) against the torch-glue HMC of tests/hmc_harness.py on the same
 fields and momenta."""
 import numpy as np
 import pytest
@@ -124,3 +124,37 @@ def test_md_with_fermion_matches_torch_hmc(cuda, hisq):
     assert abs(out["H0"] - ref["H0"]) < 1e-9 * abs(ref["H0"])
     assert abs(out["dH"] - ref["dH"]) < 1e-6 * max(1.0, abs(ref["dH"])), (out, ref)
     assert abs(out["dH_reversed"]) < 1e-5 and out["max_dU"] < 1e-7, out
+
+
+def test_omelyan_second_order_and_hmc_loop(cuda):
+    """QEX's default integrator 2MN (Omelyan): dH falls as eps^2 (halving
+    the step divides it by about 4), the trajectory reverses, and at equal
+    force evaluations its error is below leapfrog's.  The HMC loop
+    (momenta and pseudofermion heatbath, MD, Metropolis) runs and records
+    every trajectory."""
+    torch = cuda
+    from qex_b200 import md
+    dims = (8, 8, 8, 8)
+    lay = S.Layout(dims)
+    U0 = dev(F.gauge_warm(dims, 0.2, 5))
+    P0 = torch.empty_like(U0)
+    md.momenta_heatbath(lay, P0, 21, 0)
+    m = md.MD(lay, md.GaugeAction(lay, 5.6))
+    h0 = m.hamiltonian(U0, P0)
+    dh = {}
+    for integ, n in (("omelyan", 4), ("omelyan", 8), ("leapfrog", 8)):
+        U, P = U0.clone(), P0.clone()
+        m.integrate(U, P, 1.0, n, integ)
+        dh[(integ, n)] = m.hamiltonian(U, P) - h0
+        if (integ, n) == ("omelyan", 8):
+            P.neg_()
+            m.integrate(U, P, 1.0, n, integ)
+            assert abs(m.hamiltonian(U, P) - h0) < 1e-8 * abs(h0)
+            assert float((U - U0).abs().max()) < 1e-10
+    ratio = dh[("omelyan", 4)] / dh[("omelyan", 8)]
+    assert 3.0 < ratio < 5.5, dh
+    assert abs(dh[("omelyan", 4)]) < abs(dh[("leapfrog", 8)]), dh
+    ferm = md.StaggeredPseudofermion(lay, 0.2, hisq=False)
+    U, rec = md.hmc(lay, U0, 5.6, ferm, 2, nsteps=6, integrator="omelyan")
+    assert len(rec) == 2 and all(np.isfinite(r["dH"]) for r in rec)
+    assert all(0.0 < r["plaquette"] < 1.0 for r in rec)
