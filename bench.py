@@ -240,6 +240,23 @@ def timed_solves(s, yd, bd, sp_kw, steps, torch):
     return times, launches, iters, sps
 
 
+def iteration_breakdown(res, k, nh, peak, solver):
+    """Where an iteration of the fastest solve goes, from this run's live
+    times: the solve's time per iteration against the Schur operator's time
+    per call; the rest is the vector kernels (16-bit solve: 136 B per even
+    site in the update of r and x, 56 B in the p update) and the kernel
+    boundaries.  ncu, cold cache, 32^4: the update reads 46.2 MB and the p
+    update 21.0 MB per launch, their compulsory bytes; their writes stay in
+    L2 while they run."""
+    it = res["time_s"] / max(res["iterations"], 1)
+    rest = it - k["seconds"]
+    vec_bytes = {"fp16+fp64": 136 + 56, "fp32+fp64": 4 * 24 + 24 * 2 + 24 * 3, "fp64": 240 + 48 * 4}[solver]
+    return {"us_per_iteration": round(it * 1e6, 2), "schur_us": round(k["seconds"] * 1e6, 2),
+            "other_us": round(rest * 1e6, 2), "vector_bytes_per_even_site": vec_bytes,
+            "vector_GBps_if_all_other_time": round(vec_bytes * nh / max(rest, 1e-12) / 1e9, 1),
+            "vector_frac": round(vec_bytes * nh / max(rest, 1e-12) / 1e9 / peak, 4)}
+
+
 def time_multishift(s, dims, torch):
     """The mixed-precision multi-shift solve on the workload's lattice and
     fields: one Gaussian right-hand side, 12 shifts log-spaced from 1e-4 to
@@ -367,10 +384,11 @@ def run_ours(args, dims):
     peak, peak_kind = measured_peaks()
     # DRAM bytes (read + write) of one Schur call = its two half sweeps, from
     # ncu captures of these kernels at 32^4 (per-launch traffic scales with
-    # the site count)
+    # the site count); 16-bit: dslash_x2_kernel half sweep 1 260.08 MB read +
+    # 2.93 MB written, half sweep 2 268.49 + 3.95 MB (two launches each)
     ncu_traffic_32 = {"fp64": 1233229000 + 5634048 + 1258927000 + 7406080,
                       "fp32": 515961088 + 7234048 + 528527616 + 5271808,
-                      "fp16": 260101632 + 6382592 + 268475392 + 6029568}
+                      "fp16": 260084500 + 2930000 + 268494000 + 3946500}
     traffic = ncu_traffic_32[dom] * nh / 524288
     roof = {"kernel": f"Schur operator, {dom} fat+Naik (two Dslash half sweeps)", "bound": "hbm",
             "achieved": round(k["GBps"], 1), "peak": peak, "unit": "GB/s",
@@ -378,6 +396,7 @@ def run_ours(args, dims):
             "traffic": traffic, "traffic_unit": "bytes per Schur call (ncu, scaled from 32^4)",
             "bytes_per_even_site": k["bytes_per_even_site"],
             "seconds_per_call": k["seconds"],
+            "iteration": iteration_breakdown(results[best], k, nh, peak, best),
             "all_precisions": {n: {"GBps": round(v["GBps"], 1), "frac": round(v["GBps"] / peak, 4),
                                    "GFLOPs": round(v["GFLOPs"], 1), "us": round(v["seconds"] * 1e6, 1),
                                    "GBps_no_reuse": round(v["GBps_no_reuse"], 1),
