@@ -310,6 +310,9 @@ struct DslashArgsLo {
   double *partials;
   unsigned *ticket;
   double *dot_out;      // RED == 2
+  // output sites [k_lo, min(k_hi, nh)) of the parity (a domain's interior or
+  // its intermediate slices); site k is stored at index k - out_off of out
+  int k_lo = 0, k_hi = 0x7fffffff, out_off = 0;
 };
 
 template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP, int R12>
@@ -322,7 +325,8 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
   const size_t in_base = (size_t)(1 - A.po) * nh;
   const size_t out_base = (size_t)A.po * nh;
   double dot = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+  const int kend = min(nh, A.k_hi);
+  for (int k = A.k_lo + blockIdx.x * blockDim.x + threadIdx.x; k < kend; k += gridDim.x * blockDim.x) {
     int x[4], lex;
     site_coords(g, A.po, k, x, lex);
     float2 af[3], al[3], xsv[3];
@@ -395,7 +399,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
       }
       o[c] = acc;
     }
-    store_vec<OUTP>(A.out, A.ostride, k, o);
+    store_vec<OUTP>(A.out, A.ostride, k - A.out_off, o);
     if (RED) {
       float d = 0.f;
 #pragma unroll
@@ -442,7 +446,8 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
   const size_t out_base = (size_t)A.po * nh;
   const float rho = A.L.long_scale / A.L.fat_scale;
   double dot = 0.0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+  const int kend = min(nh, A.k_hi);
+  for (int k = A.k_lo + blockIdx.x * blockDim.x + threadIdx.x; k < kend; k += gridDim.x * blockDim.x) {
     int x[4], lex;
     site_coords(g, A.po, k, x, lex);
     float2 T[3], S[3], xsv[3];
@@ -508,7 +513,7 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
       acc.y = fmaf(sf, d.y, acc.y);
       o[c] = acc;
     }
-    store_vec<OUTP>(A.out, A.ostride, k, o);
+    store_vec<OUTP>(A.out, A.ostride, k - A.out_off, o);
     if (RED) {
       float dd = 0.f;
 #pragma unroll
@@ -570,19 +575,20 @@ static int lo_grid(int nh) {
 template <int PREC, int VP, int NL, int HOP, int INIT, int RED, int OUTP>
 static int launch_lo(const DslashArgsLo &A, int) {
   int grid;
+  const int nsites = std::max(0, std::min(A.g.nh, A.k_hi) - A.k_lo);
   if constexpr (PREC == kF16) {
     if (NL == 8 && A.L.recon12) {
-      grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh);
+      grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(nsites);
       launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 1>, grid, kBlock, A);
     } else {
-      grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh);
+      grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(nsites);
       launch_pdl(dslash_x2_kernel<VP, NL, HOP, INIT, RED, OUTP, 0>, grid, kBlock, A);
     }
   } else if (NL == 8 && A.L.recon12) {
-    grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(A.g.nh);
+    grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>(nsites);
     launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 1>, grid, kBlock, A);
   } else {
-    grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(A.g.nh);
+    grid = lo_grid<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>(nsites);
     launch_pdl(dslash_lo_kernel<PREC, VP, NL, HOP, INIT, RED, OUTP, 0>, grid, kBlock, A);
   }
   note_launch();
