@@ -133,7 +133,8 @@ namespace qs {
 // workspace slots of a domain's link handle
 enum DomainSlot {
   kDmIn = kSlotLast + 700, kDmOut, kDmT, kDmFull, kDmX, kDmR, kDmP, kDmAp, kDmSoa, kDmLinks,
-  kDmPack  // four NCCL z-face buffers (send down, send up, receive down, receive up)
+  kDmPack,  // four NCCL z-face buffers (send down, send up, receive down, receive up)
+  kDmMix    // five compact interior FP64 fields of the mixed-precision solve
 };
 
 // layout of a domain's device scalars (dsum): the partial sums of up to
@@ -145,6 +146,8 @@ constexpr size_t kDevScalarBytes = sizeof(double) * kStateOff + sizeof(CgState);
 
 int write_state(CgState *dst, const CgState &host);
 int check_interval(int nh);
+int build_low_links(qexstag_links_s *g);
+void free_low_links(LowLinks &low);
 
 // sites of one parity in one (z, t) row, and in one t slice of the
 // extended lattice
@@ -743,6 +746,111 @@ static int cg_iteration(qexstag_domain_s *const *ds, int n, double2 *const *xv, 
   return finish_scalar(ds, n, st, 2);
 }
 
+// ---- the mixed-precision solve on one domain per process ----
+
+struct MixedCtx {
+  qexstag_domain_s *d;
+  double2 *xe, *ae, *te;  // FP64 extended fields for the reliable updates' Schur operator
+  double m2;
+};
+
+static int mx_exchange_even(void *ctx, void *field) {
+  qexstag_domain_s *d = ((MixedCtx *)ctx)->d;
+  double2 *f = (double2 *)field;  // 16 bytes per site: one double2 component
+  return exchange(&d, 1, &f, 1, 0, stream());
+}
+
+static int mx_allreduce(void *ctx, double *dev) {
+  qexstag_domain_s *d = ((MixedCtx *)ctx)->d;
+  if (d->hostc) {
+    double *h = host_results();
+    QS_CUDA(cudaMemcpyAsync(h, dev, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+    QS_CUDA(cudaStreamSynchronize(stream()));
+    double v = h[0];
+    if (d->hc.all_reduce_sum(d->hc.ctx, &v, 1))
+      return fail(QEXSTAG_ERR_STATE, "domain: the host communicator's sum reported an error");
+    h[0] = v;
+    QS_CUDA(cudaMemcpyAsync(dev, h, sizeof(double), cudaMemcpyHostToDevice, stream()));
+    QS_CUDA(cudaStreamSynchronize(stream()));  // h is reused by the next call
+  } else if (d->comm) {
+    QS_NCCL(nccl().allReduce(dev, dev, 1, ncclDouble, ncclSum, d->comm, stream()));
+  }
+  return QEXSTAG_OK;
+}
+
+static int mx_schur64(void *ctx, const double2 *x, double2 *ax) {
+  MixedCtx *c = (MixedCtx *)ctx;
+  qexstag_domain_s *d = c->d;
+  const int ni = interior_n(d);
+  int rc;
+  if ((rc = vcopy(interior(d, c->xe), CVecD{x, ni}, ni))) return rc;
+  if ((rc = schur_set(&d, 1, &c->ae, &c->xe, &c->te, c->m2))) return rc;
+  return vcopy(VecD{ax, ni}, cv(interior(d, c->ae)), ni);
+}
+
+// FP64 defect correction (stagSolve.nim:330-421) around the 16-bit
+// reliable-update CG of cg_mixed_domain; bv: the source on the extended
+// lattice, xv: receives the solution's interior even sites.
+static int solve_mixed_domain(qexstag_domain_s *d, double2 *bv, double2 *xv, double2 *ae, double2 *te, double m,
+                              const qexstag_solver_params *p, qexstag_solver_stats *st, double *r2_out) {
+  const int ni = interior_n(d);
+  const size_t vb = sizeof(double2) * 3 * (size_t)ni;
+  void *pb, *px, *prho, *py, *pax;
+  int rc;
+  Workspace &ws = d->g->ws;
+  if ((rc = ws.get(kDmMix + 0, vb, &pb)) || (rc = ws.get(kDmMix + 1, vb, &px)) || (rc = ws.get(kDmMix + 2, vb, &prho)) ||
+      (rc = ws.get(kDmMix + 3, vb, &py)) || (rc = ws.get(kDmMix + 4, vb, &pax)))
+    return rc;
+  double2 *b = (double2 *)pb, *x = (double2 *)px, *rho = (double2 *)prho, *y = (double2 *)py, *ax = (double2 *)pax;
+  const double m2 = m * m;
+  MixedCtx ctx{d, xv, ae, te, m2};
+  const size_t eb = sizeof(double2) * 3 * (size_t)d->ext->g.V;
+  QS_CUDA(cudaMemsetAsync(xv, 0, eb, stream()));
+  MxDomain D;
+  D.ctx = &ctx;
+  D.exchange_even = mx_exchange_even;
+  D.allreduce = mx_allreduce;
+  D.schur64 = mx_schur64;
+  D.g = d->g;
+  const int sh = (int)slice_half(d), rho_hop = d->h / 2;
+  D.even_lo = d->h * sh;
+  D.n = ni;
+  D.odd_lo = (d->h - rho_hop) * sh;
+  D.odd_hi = (d->h + d->T + rho_hop) * sh;
+  if ((rc = vcopy(VecD{b, ni}, cv(interior(d, bv)), ni)) || (rc = vcopy(VecD{rho, ni}, CVecD{b, ni}, ni)) ||
+      (rc = vzero(VecD{x, ni}, ni)))
+    return rc;
+  double b2l = 0, b2 = 0;
+  if ((rc = vnorm2(CVecD{b, ni}, ni, &b2l)) || (rc = allreduce_sum(&d, 1, &b2l, &b2))) return rc;
+  if (!std::isfinite(b2)) return fail(QEXSTAG_ERR_NAN, "domain_solveEE: source is not finite");
+  double r2 = b2, r2prev = INFINITY;
+  const double r2stop = p->r2req * b2;
+  const int maxits = p->maxits > 0 ? p->maxits : 50000;
+  const double delta = p->delta > 0 ? p->delta : 0.3;
+  while (r2 > r2stop && r2 < r2prev) {
+    r2prev = r2;
+    const int mx = maxits - st->iterations;
+    if (mx <= 0) break;
+    CgOut o{};
+    int rel = 0;
+    if ((rc = cg_mixed_domain(D, m2, rho, y, r2stop / r2, mx, delta, &o, &rel))) return rc;
+    st->iterations += o.iterations;
+    st->reliable_updates += rel;
+    st->outer_iterations += 1;
+    double r2l = 0;
+    if ((rc = vaxpy(VecD{x, ni}, 1.0, CVecD{y, ni}, ni)) || (rc = mx_schur64(&ctx, x, ax)) ||
+        (rc = vsub(VecD{rho, ni}, CVecD{b, ni}, CVecD{ax, ni}, ni)) || (rc = vnorm2(CVecD{rho, ni}, ni, &r2l)) ||
+        (rc = allreduce_sum(&d, 1, &r2l, &r2)))
+      return rc;
+    if (std::isnan(r2)) return fail(QEXSTAG_ERR_NAN, "domain_solveEE: NaN residual");
+  }
+  // the solution into the extended field's interior (odd sites and ghosts zero)
+  QS_CUDA(cudaMemsetAsync(xv, 0, eb, stream()));
+  if ((rc = vcopy(interior(d, xv), CVecD{x, ni}, ni))) return rc;
+  *r2_out = r2;
+  return QEXSTAG_OK;
+}
+
 }  // namespace qs
 
 using namespace qs;
@@ -949,6 +1057,11 @@ int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const
   const int ncomp = 9 * doms[0]->nl;
   for (int par = 0; par < 2; par++)
     if ((rc = exchange(doms, n, base.data(), ncomp, par, stream()))) return rc;
+  // the reduced-precision copies the mixed-precision solve iterates with
+  for (int k = 0; k < n; k++) {
+    free_low_links(doms[k]->g->low);
+    if ((rc = build_low_links(doms[k]->g))) return rc;
+  }
   QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
 }
@@ -1014,6 +1127,42 @@ int qexstag_domain_solveEE(qexstag_domain *const *doms, int n, double *const *x,
     if ((rc = vcopy(interior(d, rv[k]), cv(interior(d, bv[k])), ni)) ||
         (rc = vcopy(interior(d, pv[k]), cv(interior(d, bv[k])), ni)))
       return rc;
+  }
+  if (p->sloppy != QEXSTAG_SLOPPY_NONE) {
+    if (p->sloppy != QEXSTAG_SLOPPY_HALF || n != 1 || doms[0]->hz > 0)
+      return fail(QEXSTAG_ERR_ARG, "domain_solveEE: a mixed-precision domain solve takes sloppy HALF, one domain "
+                                   "per call and a split along t only");
+    qexstag_domain_s *d = doms[0];
+    if (!d->g->low.ready) return fail(QEXSTAG_ERR_STATE, "domain_solveEE: set the links first");
+    qexstag_solver_stats s2;
+    std::memset(&s2, 0, sizeof s2);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, stream());
+    const long long l0 = launch_count();
+    double r2 = 0, b2 = 0;
+    rc = dot_set(doms, 1, bv.data(), bv.data(), &b2);
+    if (!rc) rc = solve_mixed_domain(d, bv[0], xv[0], ap[0], tv[0], m, p, &s2, &r2);
+    cudaEventRecord(e1, stream());
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if ((rc = vec_out(d, xv[0], x[0], mem))) return rc;
+    QS_CUDA(cudaStreamSynchronize(stream()));
+    if (st_out) {
+      *st_out = s2;
+      st_out->calls = 1;
+      st_out->seconds = ms * 1e-3;
+      st_out->flops = (double)(d->nl * 4 * 72 + 60) *
+                      ((double)d->gdims[0] * d->gdims[1] * d->gdims[2] * d->gdims[3] / 2) * s2.iterations;
+      st_out->r2 = b2 > 0 ? r2 / b2 : 0.0;
+      st_out->kernel_launches = launch_count() - l0;
+    }
+    return r2 <= p->r2req * b2 * 1.0000001 ? QEXSTAG_OK : QEXSTAG_NOT_CONVERGED;
   }
   double b2 = 0;
   if ((rc = dot_set(doms, n, bv.data(), bv.data(), &b2))) return rc;

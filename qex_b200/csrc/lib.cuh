@@ -78,6 +78,24 @@ enum RedKind { kRedNone = 0, kRedCgPAp = 1, kRedDot = 2 };
 int dslash64(const qexstag_links_s *g, int po, VecD out, CVecD xin, CVecD xs, CVecD rin,
              double a, double b, double c, int hop, int init, int red = kRedNone,
              void *state = nullptr, const int *done = nullptr, double *dot_out = nullptr);
+// One domain of a decomposed lattice for the mixed-precision CG
+// (mixed.cu: cg_mixed_domain): the links of its extended lattice, its
+// interior even sites [even_lo, even_lo + n) and the odd sites
+// [odd_lo, odd_hi) half sweep 1 must produce, and the decomposition's
+// operations: the ghost exchange of an even field of 16-byte sites, the
+// in-place sum over processes of one device double, and the FP64 Schur
+// operator on compact interior fields (double2 [3][n]).
+struct MxDomain {
+  void *ctx;
+  int (*exchange_even)(void *ctx, void *field);
+  int (*allreduce)(void *ctx, double *dev);
+  int (*schur64)(void *ctx, const double2 *x, double2 *ax);
+  qexstag_links_s *g;
+  int even_lo, n, odd_lo, odd_hi;
+};
+struct CgOut;
+int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, double r2req, int maxits,
+                    double delta, CgOut *out, int *reliable);
 // stagDN (mrhs.cu): r[i] (parity po) = m x[i] + (2D) x[i], i < n
 int dslashN64(const qexstag_links_s *gl, int po, int n, double2 *const *r, int rstride, const double2 *const *x,
               int xstride, double m);

@@ -1076,6 +1076,279 @@ int cg_mixed(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2r
   return vcopy(x, cv(xc), nh);
 }
 
+// ---------------------------------------------------------------------------
+// the 16-bit reliable-update CG on one domain of a decomposed lattice
+//
+// The same iteration as cg_mixed_t on the domain's extended lattice: half
+// sweep 1 on the odd slices the second needs ([odd_lo, odd_hi), reaching
+// rho slices into the ghosts), half sweep 2 and the vector updates on the
+// interior even sites.  Before half sweep 1 the ghost slices of p (16 bytes
+// per site) are exchanged, and every sum (<p, Ap>, |r|^2, and at reliable
+// updates |b - Ax|^2 and <r, p>) is the domain's partial, added in block
+// order, then summed over the processes, before the state kernels use it.
+// The caller provides the exchange, the sum and the FP64 Schur operator of
+// the decomposed lattice (MxDomain).
+// ---------------------------------------------------------------------------
+
+// sum of np partials into *val (one block, fixed order)
+__global__ void mxd_sum_kernel(const double *partials, int np, double *val) {
+  __shared__ double sh[32];
+  double v[1] = {0.0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v[0] += __ldcg(partials + i);
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) *val = v[0];
+}
+
+// r = b, x = 0, rs = b, xs = 0, p = b; per-block |b|^2
+template <int VP>
+__global__ void __launch_bounds__(kBlock)
+    mxd_init_kernel(const double2 *__restrict__ b, double2 *__restrict__ x, double2 *__restrict__ r,
+                    float2 *__restrict__ rs, float2 *__restrict__ xs, void *p, int n, double *partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 v = b[(size_t)c * n + i];
+      x[(size_t)c * n + i] = make_double2(0.0, 0.0);
+      r[(size_t)c * n + i] = v;
+      pv[c] = make_float2((float)v.x, (float)v.y);
+      rs[(size_t)c * n + i] = pv[c];
+      xs[(size_t)c * n + i] = make_float2(0.f, 0.f);
+      s = fma(v.x, v.x, s);
+      s = fma(v.y, v.y, s);
+    }
+    store_vec<VP>(p, n, i, pv);
+  }
+  __shared__ double sh[32];
+  double v[1] = {s};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+// the state at the start (as mx_init_kernel), from the summed |b|^2
+__global__ void mxd_init_state_kernel(MxState *st, const double *b2p) {
+  const double b2 = *b2p;
+  st->b2 = b2;
+  st->r2 = b2;
+  st->r2old = b2;
+  st->r2stop = st->r2req * b2;
+  st->rNorm = st->r0Norm = st->maxrx = st->maxrr = sqrt(b2);
+  st->itn = 0;
+  st->pending = 0;
+  st->reliable = 0;
+  st->nan = isfinite(b2) ? 0 : 1;
+  st->done = (!(b2 > st->r2stop) || st->maxits <= 0 || st->nan) ? 1 : 0;
+}
+
+// reliable update: r = b - Ax, rs = r; per-block |r|^2
+__global__ void __launch_bounds__(kBlock)
+    mxd_true_res_kernel(const double2 *__restrict__ b, const double2 *__restrict__ ax, double2 *__restrict__ r,
+                        float2 *__restrict__ rs, int n, double *partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 bv = b[(size_t)c * n + i], a = ax[(size_t)c * n + i];
+      const double2 v = make_double2(bv.x - a.x, bv.y - a.y);
+      r[(size_t)c * n + i] = v;
+      rs[(size_t)c * n + i] = make_float2((float)v.x, (float)v.y);
+      s = fma(v.x, v.x, s);
+      s = fma(v.y, v.y, s);
+    }
+  }
+  __shared__ double sh[32];
+  double v[1] = {s};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+// the decisions of mx_true_res_kernel from the summed true |r|^2
+__global__ void mxd_true_res_state_kernel(MxState *st, const double *r2p) {
+  const double r2 = *r2p;
+  st->r2 = r2;
+  st->reliable += 1;
+  if (!isfinite(r2)) {
+    st->nan = 1;
+    st->done = 1;
+    return;
+  }
+  if (r2 <= st->r2stop || st->itn >= st->maxits) {
+    st->done = 1;
+    return;
+  }
+  const double rn = sqrt(r2);
+  st->rNorm = st->r0Norm = st->maxrr = st->maxrx = rn;
+  st->beta = r2 / st->r2old;
+}
+
+// per-block <rs, p> (mx_rp_kernel without the grid reduction)
+template <int PREC>
+__global__ void __launch_bounds__(kBlock)
+    mxd_rp_kernel(const float2 *__restrict__ rs, const void *p, int n, double *partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float2 pv[3];
+    load_vec<PREC>(p, n, i, pv);
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float2 r = rs[(size_t)c * n + i];
+      acc = fmaf(r.x, pv[c].x, acc);
+      acc = fmaf(r.y, pv[c].y, acc);
+    }
+    s += (double)acc;
+  }
+  __shared__ double sh[32];
+  double v[1] = {s};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+__global__ void mxd_set_rp_kernel(MxState *st, const double *rp) {
+  if (!st->done) st->rp = *rp;
+}
+
+int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, double r2req, int maxits,
+                    double delta, CgOut *out, int *reliable) {
+  constexpr int PREC = kF16;
+  constexpr int VP = VecPrec<PREC>::v;
+  static_assert(VP == kF16, "the ghost exchange moves 16-byte sites");
+  qexstag_links_s *g = D.g;
+  if (!g->low.ready) return fail(QEXSTAG_ERR_STATE, "domain mixed cg: reduced-precision links missing");
+  const Geom &geo = g->l->g;
+  const int n = D.n, nh = geo.nh;
+  Workspace &ws = g->ws;
+  const size_t v64 = sizeof(double2) * 3 * (size_t)n, v32 = sizeof(float2) * 3 * (size_t)n;
+  void *pr, *pax, *prs, *pxs, *pap, *pp, *pt, *pst, *pval, *ppart;
+  int rc;
+  if ((rc = ws.get(kSlotMx0 + 30, v64, &pr)) || (rc = ws.get(kSlotMx0 + 31, v64, &pax)) ||
+      (rc = ws.get(kSlotMx0 + 32, v32, &prs)) || (rc = ws.get(kSlotMx0 + 33, v32, &pxs)) ||
+      (rc = ws.get(kSlotMx0 + 34, v32, &pap)) || (rc = ws.get(kSlotMx0 + 35, sizeof(uint4) * (size_t)nh, &pp)) ||
+      (rc = ws.get(kSlotMx0 + 36, sizeof(uint4) * (size_t)nh, &pt)) ||
+      (rc = ws.get(kSlotMx0 + 37, sizeof(MxState), &pst)) || (rc = ws.get(kSlotMx0 + 38, sizeof(double) * 4, &pval)) ||
+      (rc = ws.get(kSlotMx0 + 39, sizeof(double) * 2 * kMaxRedBlocks, &ppart)))
+    return rc;
+  double2 *r = (double2 *)pr, *ax = (double2 *)pax;
+  float2 *rs = (float2 *)prs, *xs = (float2 *)pxs, *ap = (float2 *)pap;
+  uint4 *p = (uint4 *)pp, *t = (uint4 *)pt;
+  uint4 *pin = p + D.even_lo;  // the interior part of p, compact
+  MxState *st = (MxState *)pst;
+  double *val = (double *)pval, *part = (double *)ppart, *part2 = part + kMaxRedBlocks;
+  // zero p and t so that sites no sweep writes hold finite values
+  QS_CUDA(cudaMemsetAsync(p, 0, sizeof(uint4) * (size_t)nh, stream()));
+  QS_CUDA(cudaMemsetAsync(t, 0, sizeof(uint4) * (size_t)nh, stream()));
+  MxState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.r2req = r2req;
+  hs.maxits = maxits;
+  hs.delta = delta;
+  {
+    double *buf = host_results();
+    std::memcpy(buf, &hs, sizeof(hs));
+    QS_CUDA(cudaMemcpyAsync(st, buf, sizeof(hs), cudaMemcpyHostToDevice, stream()));
+    QS_CUDA(cudaStreamSynchronize(stream()));
+  }
+  const int grid = std::min(grid_for(n, kBlock, 4), kMaxRedBlocks);
+  const int egrid = grid_for(n, kBlock, 8);
+  // the summed value at val[0], over processes
+  auto sum_over = [&](const double *partials, int np) -> int {
+    mxd_sum_kernel<<<1, kBlock, 0, stream()>>>(partials, np, val);
+    note_launch();
+    QS_LAUNCH_CHECK();
+    return D.allreduce(D.ctx, val);
+  };
+  mxd_init_kernel<VP><<<grid, kBlock, 0, stream()>>>(b, x, r, rs, xs, pin, n, part);
+  note_launch();
+  QS_LAUNCH_CHECK();
+  if ((rc = sum_over(part, grid))) return rc;
+  mxd_init_state_kernel<<<1, 1, 0, stream()>>>(st, val);
+  note_launch();
+  DslashArgsLo A1, A2;
+  A1.g = geo;
+  A1.L = lo_links(g->low, PREC);
+  A1.halt = st;
+  A1.state = st;
+  A1.partials = part;
+  A1.ticket = red_tickets();
+  A1.dot_out = nullptr;
+  A1.po = 1;
+  A1.xin = p;
+  A1.istride = nh;
+  A1.xs = nullptr;
+  A1.sstride = 0;
+  A1.out = t;
+  A1.ostride = nh;
+  A1.b = 0.f;
+  A1.k_lo = D.odd_lo;
+  A1.k_hi = D.odd_hi;
+  A2 = A1;
+  A2.po = 0;
+  A2.xin = t;
+  A2.xs = p;
+  A2.sstride = nh;
+  A2.out = ap;
+  A2.ostride = n;
+  A2.out_off = D.even_lo;
+  A2.b = (float)(4.0 * m2);
+  A2.k_lo = D.even_lo;
+  A2.k_hi = D.even_lo + n;
+  auto iteration = [&]() -> int {
+    int rc2 = D.exchange_even(D.ctx, p);
+    if (rc2) return rc2;
+    int np = 0;
+    if ((rc2 = g->nl == 8 ? sloppy_half<PREC, 8>(0, A1, 0, 0, nullptr) : sloppy_half<PREC, 4>(0, A1, 0, 0, nullptr)))
+      return rc2;
+    if ((rc2 = g->nl == 8 ? sloppy_half<PREC, 8>(1, A2, 0, 3, &np) : sloppy_half<PREC, 4>(1, A2, 0, 3, &np)))
+      return rc2;
+    if ((rc2 = sum_over(part, np))) return rc2;
+    launch_pdl(mx_update_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)pin, n, st,
+               (const double *)val, 1, part2);
+    note_launch();
+    if ((rc2 = sum_over(part2, grid))) return rc2;
+    launch_pdl(mx_p_kernel<VP>, egrid, kBlock, (const float2 *)rs, (void *)pin, n, st, (const double *)val, 1);
+    note_launch();
+    QS_LAUNCH_CHECK();
+    return QEXSTAG_OK;
+  };
+  auto reliable_update = [&]() -> int {
+    mx_flush_kernel<<<egrid, kBlock, 0, stream()>>>(x, xs, n);
+    note_launch();
+    int rc2 = D.schur64(D.ctx, x, ax);
+    if (rc2) return rc2;
+    mxd_true_res_kernel<<<grid, kBlock, 0, stream()>>>(b, ax, r, rs, n, part);
+    note_launch();
+    if ((rc2 = sum_over(part, grid))) return rc2;
+    mxd_true_res_state_kernel<<<1, 1, 0, stream()>>>(st, val);
+    mxd_rp_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, pin, n, part);
+    note_launch(2);
+    if ((rc2 = sum_over(part, grid))) return rc2;
+    mxd_set_rp_kernel<<<1, 1, 0, stream()>>>(st, val);
+    mx_p_reliable_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, pin, n, st);
+    mx_clear_pending_kernel<<<1, 1, 0, stream()>>>(st);
+    note_launch(3);
+    QS_LAUNCH_CHECK();
+    return QEXSTAG_OK;
+  };
+  // every process sees the same summed state, so all run the same batches
+  // (kernels past convergence or a pending update return at once)
+  const int every = check_interval(n);
+  StateSnapshot snap;
+  for (;;) {
+    for (int i = 0; i < every; i++)
+      if ((rc = iteration())) return rc;
+    if ((rc = snap.start(st, sizeof(MxState))) || (rc = snap.wait(&hs, sizeof(MxState)))) return rc;
+    if (hs.done) break;
+    if (hs.pending && (rc = reliable_update())) return rc;
+  }
+  out->iterations = hs.itn;
+  out->r2 = hs.b2 > 0 ? hs.r2 / hs.b2 : 0.0;
+  out->nan = hs.nan;
+  *reliable = hs.reliable;
+  if (hs.nan) return fail(QEXSTAG_ERR_NAN, "domain mixed cg: NaN in residual");
+  return QEXSTAG_OK;
+}
+
 }  // namespace qs
 
 // ---------------------------------------------------------------------------

@@ -50,8 +50,13 @@ def _worker(rank, world, port, q, dims, grid):
         y = np.zeros_like(b)
         sp = S.SolverParams(r2req=1e-20)
         d.solveEE(y, b, M, sp)
+        y16 = np.zeros_like(b)
+        sp16 = S.SolverParams(r2req=1e-20, sloppySolve=S.L.SLOPPY_HALF, delta=0.1)
+        if grid is None:  # the 16-bit domain solve: splits along t
+            d.solveEE(y16, b, M, sp16)
         ix = d.gidx[0]
-        q.put((rank, ix, r[ix], y[ix], sp.iterations, sp.r2, sp.status))
+        q.put((rank, ix, r[ix], y[ix], sp.iterations, sp.r2, sp.status, y16[ix], sp16.r2, sp16.status,
+               sp16.reliable_updates))
         del d
     finally:
         dist.destroy_process_group()
@@ -79,10 +84,14 @@ def test_two_process_domain_solve(cuda, dims, grid):
     x[V // 2:] = 0
     r = np.zeros_like(x)
     y = np.zeros_like(b)
-    for rank, ix, rp, yp, its, r2, status in out:
+    y16 = np.zeros_like(b)
+    for rank, ix, rp, yp, its, r2, status, y16p, r216, st16, rel16 in out:
         r[ix] = rp
         y[ix] = yp
+        y16[ix] = y16p
         assert status == 0 and r2 <= 1e-20
+        if grid is None:
+            assert st16 == 0 and r216 <= 1e-20 and rel16 >= 1
     # the Schur operator: bit for bit the single-lattice one
     s = S.Staggered(S.Layout(dims), g)
     r1 = np.zeros_like(x)
@@ -94,3 +103,37 @@ def test_two_process_domain_solve(cuda, dims, grid):
     its_o, _ = o.solveXX(0, yo, b, M, 1e-20)
     assert out[0][4] == out[1][4] and abs(out[0][4] - its_o) <= 1
     assert np.abs(y - yo).max() / np.abs(yo).max() < 1e-8
+    if grid is None:
+        # the 16-bit reliable-update CG over the two processes, FP64 defect
+        # correction: the oracle's solution and the FP64 true residual
+        assert np.abs(y16 - yo).max() / np.abs(yo).max() < 1e-8
+        ay = o.vec()
+        o.stagD2ee(ay, y16, M * M)
+        assert np.linalg.norm(ay[: V // 2] - b[: V // 2]) ** 2 <= 1e-20 * np.linalg.norm(b[: V // 2]) ** 2
+        assert not np.any(y16[V // 2:])
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8, 8), (8, 4, 6, 12)])
+def test_one_domain_mixed_solve(cuda, dims):
+    """The 16-bit domain solve with one domain holding the whole lattice
+    (its ghosts exchanged with itself): the oracle's solution, the FP64
+    true residual, and the error reported for what it does not take."""
+    from oracle import oracle as O
+    from qex_b200 import domain as DD
+    from qex_b200 import fields as F
+    from qex_b200 import stag as S
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 23)
+    b = F.even_source(dims, 24)
+    d = DD.DomainSet(dims, 1, 8)
+    d.set_links(g)
+    y = np.zeros_like(b)
+    sp = S.SolverParams(r2req=1e-20, sloppySolve=S.L.SLOPPY_HALF, delta=0.1)
+    d.solveEE(y, b, M, sp)
+    assert sp.status == 0 and sp.r2 <= 1e-20 and sp.reliable_updates >= 1
+    o = O.Oracle(dims, g)
+    yo = o.vec()
+    o.solveXX(0, yo, b, M, 1e-22)
+    assert np.abs(y - yo).max() / np.abs(yo).max() < 1e-8
+    with pytest.raises(S.L.QexStagError):
+        d.solveEE(y, b, M, S.SolverParams(r2req=1e-20, sloppySolve=S.L.SLOPPY_SINGLE))
