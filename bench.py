@@ -11,8 +11,10 @@ solve through the C ABI with host (QEX-layout) buffers, copies included.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--dims 32,32,32,32]
 
-With N > 1 (torchrun) every rank solves its own replica (the solve does not
-shard across GPUs here); timing is the max over ranks.
+With N > 1 (torchrun) the lattice grows with N: 32^3 x (32 N), split along
+t into one 32^4 slab per GPU and solved by the domain decomposition's
+16-bit CG with NCCL exchanges (weak scaling; --replicas: one independent
+32^4 solve per GPU instead); timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -100,9 +102,11 @@ class ClockSampler:
 
 
 def dist_setup(backend="nccl"):
-    """One process per GPU (torchrun): every rank solves its own replica, so
-    the only collectives are the barriers around the timed region and the
-    max over ranks of the timings."""
+    """One process per GPU (torchrun).  The process group carries the
+    barriers around the timed region and the max over ranks of the timings;
+    for the domain split also the broadcast of the NCCL id (the library's
+    own communicator does the exchanges), or, over gloo, the exchanges
+    themselves."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -331,14 +335,124 @@ def time_stagdn(s, nh, torch, peak):
     return out
 
 
+def run_domain(args, dims, ws, rank, local):
+    """N > 1: one lattice of dims[0] x dims[1] x dims[2] x (dims[3] N) split
+    along t into N slabs of dims, one per rank (weak scaling), solved by the
+    domain decomposition's 16-bit reliable-update CG (delta 0.1, FP64 defect
+    correction) with its ghost exchanges and sums over NCCL (one GPU per
+    rank) or, with --transport host, through host memory over the process
+    group (gloo).  Each rank draws its own slab of the fat+Naik field (its
+    seed, phases from global coordinates) and of the source.  value: max
+    over ranks of the mean device time to solution."""
+    import torch
+    import torch.distributed as dist
+
+    from qex_b200 import domain as DD
+    from qex_b200 import fields as F
+    from qex_b200 import stag as S
+    gdims = (dims[0], dims[1], dims[2], dims[3] * ws)
+    off = (0, 0, 0, dims[3] * rank)
+    if args.transport == "nccl":
+        obj = [DD.nccl_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(obj, src=0)
+        d = DD.DomainSet(gdims, ws, 8, ranks=[rank], nccl_id=obj[0], device=local)
+    else:
+        d = DD.DomainSet(gdims, ws, 8, ranks=[rank], host_comm=DD.TorchHostComm(), device=local)
+    S.set_stream(torch.cuda.current_stream().cuda_stream)
+    g = F.fat_naik_slab(gdims, dims, off, 21 + 1000 * rank)
+    d.set_links_local([S.to_device_links(g)])
+    b_h = F.even_source(dims, 31 + 1000 * rank)
+    bd = S.to_device_vector(b_h)
+    xd = torch.zeros_like(bd)
+
+    def solve(kw):
+        sp = S.SolverParams(r2req=R2REQ, **kw)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d.solveEE_local([xd], [bd], MASS, sp)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3, sp
+
+    kw16 = {"sloppySolve": 2, "delta": DELTA}
+    for _ in range(args.warmup):
+        solve(kw16)
+    barrier(ws)
+    torch.cuda.synchronize()
+    times, launches = [], 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t, sp = solve(kw16)
+            times.append(t)
+            launches += sp.kernel_launches
+    torch.cuda.synchronize()
+    barrier(ws)
+    value = max_over_ranks(float(np.mean(times)), ws)
+    its16, r216 = sp.iterations, sp.r2
+    t64, sp64 = solve({"sloppySolve": 0})
+    t64 = max_over_ranks(t64, ws)
+    # e2e: host buffers in the rank's local V=1 order, copies in the timed region
+    bh = np.ascontiguousarray(b_h)
+    xh = np.zeros_like(bh)
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        sp = S.SolverParams(r2req=R2REQ, **kw16)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d.solveEE_local([xh], [bh], MASS, sp)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e = max_over_ranks(float(np.mean(e2e_times)), ws)
+    # roofline of the dominant kernel on this rank's slab (the 16-bit Schur
+    # operator of the slab's links; the domain solve runs the same kernel on
+    # the slab and its ghost slices)
+    from qex_b200.kernel_timing import time_schur
+    s = S.Staggered(S.Layout(dims), S.to_device_links(g))
+    nh = F.volume(dims) // 2
+    k = time_schur(s, nh, (2,), nrep=20)["fp16"]
+    peak, peak_kind = measured_peaks()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp16+fp64",
+                "data": "synthetic (seeded numpy per rank: warmSU(0.3) links, Gaussian source)",
+                "config": {**config_dict(gdims),
+                           "workload": f"fat+Naik staggered even-odd CG, {'x'.join(map(str, gdims))} split along t "
+                                       f"into {ws} slabs of {'x'.join(map(str, dims))}, m={MASS}, "
+                                       f"Gaussian even source, true r2 <= 1e-20 |b|^2",
+                           "parallelism": f"domain decomposition along t, {ws} ranks, {args.transport} exchange"},
+                "solver": "fp16+fp64 (domain)", "iterations": its16, "true_r2": r216,
+                "fp64_domain_time_s": t64, "fp64_domain_iterations": sp64.iterations,
+                "speedup_vs_fp64": t64 / value,
+                "roofline": {"kernel": "Schur operator, fp16 fat+Naik, one rank's slab", "bound": "hbm",
+                             "achieved": round(k["GBps"], 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(k["GBps"] / peak, 4), "peak_source": peak_kind, "traffic": None,
+                             "bytes_per_even_site": k["bytes_per_even_site"], "seconds_per_call": k["seconds"]},
+                "cpu_baseline": None,
+                "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(bh.nbytes) // 2,
+                        "d2h_bytes_per_step": int(xh.nbytes), "host_memory": "pageable", "per_rank": True},
+                "clocks": clk.summary(), "gpu_launches": int(launches)}
+        print(json.dumps(line), flush=True)
+    del s
+    del d
+
+
 def run_ours(args, dims):
     import torch
 
     from qex_b200 import fields as F
     from qex_b200 import stag as S
-    ws, rank, local = dist_setup()
+    ws, rank, local = dist_setup("gloo" if args.transport == "host" else "nccl")
+    local = local % max(1, torch.cuda.device_count())
     torch.cuda.set_device(local)
     S.init(local)
+    if ws > 1 and not args.replicas:
+        run_domain(args, dims, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     S.set_stream(torch.cuda.current_stream().cuda_stream)
     g, b = make_inputs(dims, rank)
     V = F.volume(dims)
@@ -472,6 +586,10 @@ def main():
     ap.add_argument("--ref-maxits", type=int, default=100000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-multishift", action="store_true", help="skip the multi-shift comparison")
+    ap.add_argument("--transport", default="nccl", choices=["nccl", "host"],
+                    help="N > 1: domain exchanges over NCCL, or through host memory over gloo")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: one independent 32^4 solve per GPU instead of the domain split")
     args = ap.parse_args()
     dims = tuple(int(v) for v in args.dims.split(","))
     if args.impl == "reference":

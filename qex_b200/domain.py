@@ -182,6 +182,28 @@ class DomainSet:
                                               _arr([a.ctypes.data for a in self._links]), L.MEM_HOST),
                 "domain_links")
 
+    def set_links_local(self, parts) -> None:
+        """Each domain's links in its local V=1 order, (nlinks, Vloc, 3, 3)
+        host arrays or (nlinks, 3, 3, Vloc) device tensors, phases folded in
+        with global coordinates."""
+        self._links = list(parts)
+        ptrs, mem = zip(*[S._ptr(a) for a in self._links])
+        if len(set(mem)) != 1:
+            raise ValueError("mixing host and device links")
+        L.check(self.lib.qexstag_domain_links(self._set(), len(self.handles), _arr([p.value for p in ptrs]), mem[0]),
+                "domain_links")
+
+    def solveEE_local(self, xs, bs, m: float, sp: S.SolverParams) -> None:
+        """solveEE with each domain's fields in its local V=1 order (host
+        (Vloc, 3) arrays or device (3, Vloc) tensors)."""
+        mem = S._mem_of(*xs, *bs)
+        st = L.SolverStatsC()
+        pc = sp.c_params()
+        rc = self.lib.qexstag_domain_solveEE(self._set(), len(self.handles), _arr([S._ptr(a, True)[0].value for a in xs]),
+                                             _arr([S._ptr(a)[0].value for a in bs]), m, C.byref(pc), C.byref(st), mem)
+        L.check(rc, "domain_solveEE")
+        sp.take(st, rc)
+
     def stagD2ee(self, r: np.ndarray, x: np.ndarray, m2: float) -> None:
         xs = self.split_vector(x)
         rs = self.split_vector(r)

@@ -177,6 +177,28 @@ def fat_naik_links(dims, seed: int = 21) -> np.ndarray:
     return apply_phases(dims, interleave(fat, lng))
 
 
+def fat_naik_slab(global_dims, local_dims, offset, seed: int) -> np.ndarray:
+    """A rank's part of a fat+Naik field of the fat_naik_links recipe: links
+    of the local lattice local_dims, whose site at local coordinates x is the
+    global site x + offset, drawn with this rank's seed and phased with the
+    global coordinates (the antiperiodic boundary at the global last time
+    slice); (8, Vloc, 3, 3) in the local V=1 order.  With local_dims =
+    global_dims and offset 0 it is fat_naik_links(global_dims, seed)."""
+    rng = np.random.default_rng(seed)
+    V = volume(local_dims)
+    fat = fat_from_su3(warm_su3(4 * V, 0.3, rng), rng).reshape(4, V, 3, 3)
+    lng = warm_su3(4 * V, 0.3, rng).reshape(4, V, 3, 3)
+    g = interleave(fat, lng)
+    xg = coords(local_dims) + np.asarray(offset, dtype=np.int64)
+    for k in range(8):
+        mu, hop = k // 2, (3 if k % 2 else 1)
+        s = eta(mu, xg)
+        if mu == 3:
+            s = np.where(xg[:, 3] + hop >= global_dims[3], -s, s)
+        g[k] *= s[:, None, None]
+    return g
+
+
 def even_source(dims, seed: int = 31) -> np.ndarray:
     """Gaussian source on even sites, zero on odd sites, (V, 3)."""
     V = volume(dims)

@@ -86,3 +86,24 @@ def test_rank_sites_partition_the_lattice(gdims, grid):
         gi = rank_sites(gdims, ldims, grid, r)
         # V=1 order: the first half of each lattice is even
         assert np.all((gi[: Vl // 2] < V // 2)) and np.all(gi[Vl // 2:] >= V // 2)
+
+
+def test_fat_naik_slab_phases():
+    """A rank's slab of the fat+Naik field carries the phases of its global
+    sites; the whole lattice as one slab is fat_naik_links itself."""
+    gdims = (4, 4, 4, 12)
+    assert np.array_equal(F.fat_naik_slab(gdims, gdims, (0, 0, 0, 0), 21), F.fat_naik_links(gdims, 21))
+    ldims = (4, 4, 4, 6)
+    for r in range(2):
+        off = (0, 0, 0, 6 * r)
+        g = F.fat_naik_slab(gdims, ldims, off, 21 + r)
+        # undo the phases with the global signs: what is left is unphased, the
+        # same draws as the slab's own unphased links
+        raw = F.fat_naik_slab(ldims, ldims, (0, 0, 0, 0), 21 + r)
+        raw = F.apply_phases(ldims, raw)  # apply_phases twice = identity: raw is now unphased
+        from qex_b200.domain import rank_sites
+        gi = rank_sites(gdims, ldims, (1, 2), r)
+        for k in range(8):
+            mu, hop = k // 2, (3 if k % 2 else 1)
+            sg = F.link_signs(gdims, mu, hop)[gi]
+            assert np.array_equal(g[k], raw[k] * sg[:, None, None])
