@@ -87,6 +87,15 @@ def test_nccl_self_exchange(cuda):
     local.solveEE(ya, src, 0.2, spa)
     viaccl.solveEE(yb, src, 0.2, spb)
     assert spa.iterations == spb.iterations and np.array_equal(ya, yb)
+    # the 16-bit domain solve: the ghost exchange of p through ncclSend /
+    # ncclRecv and every sum through ncclAllReduce give the in-process result
+    ya, yb = np.zeros_like(src), np.zeros_like(src)
+    spa = S.SolverParams(r2req=1e-18, sloppySolve=S.L.SLOPPY_HALF, delta=0.1)
+    spb = S.SolverParams(r2req=1e-18, sloppySolve=S.L.SLOPPY_HALF, delta=0.1)
+    local.solveEE(ya, src, 0.2, spa)
+    viaccl.solveEE(yb, src, 0.2, spb)
+    assert spa.iterations == spb.iterations and np.array_equal(ya, yb)
+    assert spb.r2 <= 1e-18 and spb.reliable_updates >= 1
 
 
 def test_domain_errors(cuda):
