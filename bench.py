@@ -247,14 +247,14 @@ def timed_solves(s, yd, bd, sp_kw, steps, torch):
 def iteration_breakdown(res, k, nh, peak, solver):
     """Where an iteration of the fastest solve goes, from this run's live
     times: the solve's time per iteration against the Schur operator's time
-    per call; the rest is the vector kernels (16-bit solve: 136 B per even
-    site in the update of r and x, 56 B in the p update) and the kernel
-    boundaries.  ncu, cold cache, 32^4: the update reads 46.2 MB and the p
-    update 21.0 MB per launch, their compulsory bytes; their writes stay in
-    L2 while they run."""
+    per call; the rest is the fused update of r, x and p (16-bit solve: r,
+    Ap, x in FP32 and p in 16 bits read, r, x and the next p written, 152 B
+    per even site), the reliable updates spread over the iterations, and
+    the kernel boundaries."""
     it = res["time_s"] / max(res["iterations"], 1)
     rest = it - k["seconds"]
-    vec_bytes = {"fp16+fp64": 136 + 56, "fp32+fp64": 4 * 24 + 24 * 2 + 24 * 3, "fp64": 240 + 48 * 4}[solver]
+    vec_bytes = {"fp16+fp64": 3 * 24 + 16 + 2 * 24 + 16, "fp32+fp64": 4 * 24 + 3 * 24,
+                 "fp64": 240 + 48 * 4}[solver]
     return {"us_per_iteration": round(it * 1e6, 2), "schur_us": round(k["seconds"] * 1e6, 2),
             "other_us": round(rest * 1e6, 2), "vector_bytes_per_even_site": vec_bytes,
             "vector_GBps_if_all_other_time": round(vec_bytes * nh / max(rest, 1e-12) / 1e9, 1),

@@ -526,6 +526,10 @@ int qexstag_domain_connect_host(qexstag_domain *d, const qexstag_host_comm *comm
 /* Set each domain's links (links[k] for doms[k]) and exchange their
    boundary slices. */
 int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const *links, int mem);
+/* 1 when the domain's reduced-precision long links are stored with 12
+   reals (their signs rebuilt from global coordinates), 0 otherwise or
+   before qexstag_domain_links. */
+int qexstag_domain_recon12(const qexstag_domain *d);
 /* stagD2ee on the decomposed lattice: r[k] even sites from x[k]. */
 int qexstag_domain_stagD2ee(qexstag_domain *const *doms, int n, double *const *r, const double *const *x, double m2,
                             int mem);

@@ -155,6 +155,7 @@ SIGNATURES = {
     "qexstag_domain_create_zt": (I, [C.POINTER(C.c_int), C.POINTER(C.c_int), I, I, C.POINTER(P)]),
     "qexstag_domain_destroy": (I, [P]),
     "qexstag_domain_local_dims": (I, [P, C.POINTER(C.c_int)]),
+    "qexstag_domain_recon12": (I, [P]),
     "qexstag_domain_connect_local": (I, [PP, I]),
     "qexstag_nccl_unique_id": (I, [P]),
     "qexstag_domain_connect_nccl": (I, [P, P]),

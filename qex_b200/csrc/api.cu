@@ -217,6 +217,8 @@ int qexstag_layout_create(const int dims[4], qexstag_layout **out) {
   for (int d = 1; d < 4; d++) l->g.stride[d] = l->g.stride[d - 1] * dims[d - 1];
   l->g.V = (int)V;
   l->g.nh = (int)(V / 2);
+  l->g.t0 = 0;
+  l->g.L3g = dims[3];
   set_fastdiv(l->g);
   cudaGetDevice(&l->device);
   *out = l;

@@ -898,6 +898,10 @@ static int domain_create(const int global_dims[4], int Rz, int Rt, int rank, int
     delete d;
     return rc;
   }
+  // the slab's long links carry the global antiperiodic boundary: the
+  // 12-real check and the sloppy kernels' long-link signs use global time
+  le->g.t0 = d->rt * T - h;
+  le->g.L3g = global_dims[3];
   d->ext = le;
   d->local.push_back(ll->g);
   qexstag_layout_destroy(ll);
@@ -1065,6 +1069,8 @@ int qexstag_domain_links(qexstag_domain *const *doms, int n, const double *const
   QS_CUDA(cudaStreamSynchronize(stream()));
   return QEXSTAG_OK;
 }
+
+int qexstag_domain_recon12(const qexstag_domain *d) { return (d && d->g && d->g->low.recon12) ? 1 : 0; }
 
 int qexstag_domain_stagD2ee(qexstag_domain *const *doms, int n, double *const *r, const double *const *x, double m2,
                             int mem) {

@@ -31,6 +31,10 @@ struct Geom {
   // shf = log2(L) - 1 when L is a power of two (set by set_fastdiv)
   unsigned mag[3];
   int shf[3];
+  // time slice x3 of this lattice is slice (x3 + t0) mod L3g of the lattice
+  // whose antiperiodic boundary the folded phases carry: 0 and L[3] for a
+  // whole lattice; a domain's extended slab sets its own offset
+  int t0, L3g;
 };
 
 inline void set_fastdiv(Geom &g) {

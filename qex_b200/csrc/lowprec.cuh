@@ -55,18 +55,26 @@ struct LoLinks {
 // Staggered phase sign of a long link of direction mu at x (forward) and at
 // x - 3 mu (backward): eta_mu(x) (QEX phases [8,9,11,0]; eta_mu does not
 // depend on x_mu) times -1 where the three-hop link crosses the
-// antiperiodic time boundary.
+// antiperiodic time boundary.  On a domain's slab the boundary is the
+// global one: slice x3 is global slice (x3 + t0) mod L3g (t0 is even, so
+// eta is the same in either coordinate).
 __device__ __forceinline__ float eta_sign(int mu, const int x[4]) {
   int s = (mu == 0) ? x[3] : (mu == 1) ? (x[0] + x[3]) : (mu == 2) ? (x[0] + x[1] + x[3]) : 0;
   return (s & 1) ? -1.f : 1.f;
 }
+__device__ __forceinline__ int global_t(const Geom &g, int x3) {
+  int t = x3 + g.t0;
+  if (t >= g.L3g) t -= g.L3g;
+  if (t < 0) t += g.L3g;
+  return t;
+}
 __device__ __forceinline__ float long_sign_fwd(const Geom &g, const int x[4], int mu) {
   float s = eta_sign(mu, x);
-  return (mu == 3 && x[3] + 3 >= g.L[3]) ? -s : s;
+  return (mu == 3 && global_t(g, x[3]) + 3 >= g.L3g) ? -s : s;
 }
 __device__ __forceinline__ float long_sign_bck(const Geom &g, const int x[4], int mu) {
   float s = eta_sign(mu, x);
-  return (mu == 3 && x[3] < 3) ? -s : s;
+  return (mu == 3 && global_t(g, x[3]) < 3) ? -s : s;
 }
 
 // row 2 = k * conj(row0 x row1)

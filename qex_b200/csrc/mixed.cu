@@ -265,10 +265,76 @@ struct MxState {
   double alpha, beta, pAp, rp;
   double b2, r2req, r2stop, delta;
   double rNorm, r0Norm, maxrx, maxrr;
-  int itn, maxits, done, pending, nan, reliable, pad[2];
+  int itn, maxits, done, pending, nan, reliable;
+  int pin;     // p buffer (0 or 1) the last fused update read: the direction a reliable update corrects
+  int itc[2];  // iterations done, as the fused update of host parity c reads (itc[c]) and writes (itc[c ^ 1])
+  int pad;
 };
 
 __device__ __forceinline__ bool mx_halt(const MxState *st) { return st->done || st->pending; }
+
+// Layout of the reduction scratch (red_partials) in the mixed CG: per-block
+// <p, Ap> partials from 0, the update's |r|^2 partials from kMxR2, the half
+// sweep's |Ap|^2 partials from kMxApAp, the fused update's second set of
+// |r|^2 partials from kMxR2b (it reads one set and writes the other)
+constexpr int kMxR2 = kMaxRedBlocks, kMxApAp = 2 * kMaxRedBlocks, kMxR2b = 3 * kMaxRedBlocks;
+
+// The reliable-update test of the iterated |r|^2 = r2 after itn
+// iterations (one thread): |r| against delta times the largest |r| since
+// the last update (QUDA-style reliable updates), the stop at r2stop or
+// maxits, a NaN.  Returns whether the iteration goes on.  Block 0 records
+// r2, rNorm, maxrr, maxrx and the pending or NaN flags.  The fields other
+// blocks read are not written here (r0Norm, delta, r2stop, maxits) or are
+// maxima that come out the same whether read before or after block 0's
+// write (maxrr, maxrx).
+__device__ __forceinline__ bool mx_test(MxState *st, double r2, int itn) {
+  if (!isfinite(r2)) {
+    if (blockIdx.x == 0) {
+      st->r2 = r2;
+      st->nan = 1;
+      st->done = 1;
+    }
+    return false;
+  }
+  const double rn = sqrt(r2);
+  const double maxrr = fmax(st->maxrr, rn), maxrx = fmax(st->maxrx, rn);
+  const bool ux = rn < st->delta * st->r0Norm && st->r0Norm <= maxrx;
+  const bool ur = (rn < st->delta * maxrr && st->r0Norm <= maxrr) || ux;
+  const bool pend = ur || r2 <= st->r2stop || itn >= st->maxits;
+  if (blockIdx.x == 0) {
+    st->r2 = r2;
+    st->rNorm = rn;
+    st->maxrr = maxrr;
+    st->maxrx = maxrx;
+    if (pend) st->pending = 1;
+  }
+  return !pend;
+}
+
+// |r|^2 from the update's np per-block partials at r2p (added in the same
+// order by every block), then mx_test; *beta_out = r2 / r2old (recorded by
+// block 0 when the iteration goes on).  itn and r2old are not written in
+// the kernels that call this.
+__device__ __forceinline__ bool mx_decide(MxState *st, const double *r2p, int np, float *beta_out) {
+  __shared__ float sh_beta;
+  __shared__ int sh_go;
+  if (threadIdx.x < 32) {
+    double r2 = 0.0;
+    for (int i = threadIdx.x; i < np; i += 32) r2 += __ldcg(r2p + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+    if (threadIdx.x == 0) {
+      const bool go = mx_test(st, r2, st->itn);
+      const double beta = go ? r2 / st->r2old : 0.0;
+      if (go && blockIdx.x == 0) st->beta = beta;
+      sh_beta = (float)beta;
+      sh_go = go ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  if (beta_out) *beta_out = sh_beta;
+  return sh_go != 0;
+}
 
 // ---------------------------------------------------------------------------
 // sloppy Dslash: out = b*xs + hop * sum_k [...]; fat and long partial sums
@@ -325,6 +391,7 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
   const size_t in_base = (size_t)(1 - A.po) * nh;
   const size_t out_base = (size_t)A.po * nh;
   double dot = 0.0;
+  float fdot = 0.f, fdot2 = 0.f;
   const int kend = min(nh, A.k_hi);
   for (int k = A.k_lo + blockIdx.x * blockDim.x + threadIdx.x; k < kend; k += gridDim.x * blockDim.x) {
     int x[4], lex;
@@ -400,14 +467,29 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
       o[c] = acc;
     }
     store_vec<OUTP>(A.out, A.ostride, k - A.out_off, o);
-    if (RED) {
+    if (RED == 4) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        fdot = fmaf(xsv[c].x, o[c].x, fmaf(xsv[c].y, o[c].y, fdot));
+        fdot2 = fmaf(o[c].x, o[c].x, fmaf(o[c].y, o[c].y, fdot2));
+      }
+    } else if (RED) {
       float d = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; c++) d += xsv[c].x * o[c].x + xsv[c].y * o[c].y;
       dot += (double)d;
     }
   }
-  if (RED == 3) {
+  if (RED == 4) {
+    // per-block partials of Re <xs, out> (from 0) and |out|^2 (from kMxApAp)
+    __shared__ double sh4[64];
+    double v[2] = {(double)fdot, (double)fdot2};
+    block_sum<2>(v, sh4);
+    if (threadIdx.x == 0) {
+      A.partials[blockIdx.x] = v[0];
+      A.partials[kMxApAp + blockIdx.x] = v[1];
+    }
+  } else if (RED == 3) {
     __shared__ double sh3[32];
     double v[1] = {dot};
     block_sum<1>(v, sh3);
@@ -446,6 +528,7 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
   const size_t out_base = (size_t)A.po * nh;
   const float rho = A.L.long_scale / A.L.fat_scale;
   double dot = 0.0;
+  float fdot = 0.f, fdot2 = 0.f;
   const int kend = min(nh, A.k_hi);
   for (int k = A.k_lo + blockIdx.x * blockDim.x + threadIdx.x; k < kend; k += gridDim.x * blockDim.x) {
     int x[4], lex;
@@ -514,14 +597,30 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
       o[c] = acc;
     }
     store_vec<OUTP>(A.out, A.ostride, k - A.out_off, o);
-    if (RED) {
+    if (RED == 4) {
+      // FP32 per thread (a thread holds one or two sites): two registers
+      // fewer than FP64 sums, which the 64-register budget needs
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        fdot = fmaf(xsv[c].x, o[c].x, fmaf(xsv[c].y, o[c].y, fdot));
+        fdot2 = fmaf(o[c].x, o[c].x, fmaf(o[c].y, o[c].y, fdot2));
+      }
+    } else if (RED) {
       float dd = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; c++) dd += xsv[c].x * o[c].x + xsv[c].y * o[c].y;
       dot += (double)dd;
     }
   }
-  if (RED == 3) {
+  if (RED == 4) {
+    __shared__ double sh4[64];
+    double v[2] = {(double)fdot, (double)fdot2};
+    block_sum<2>(v, sh4);
+    if (threadIdx.x == 0) {
+      A.partials[blockIdx.x] = v[0];
+      A.partials[kMxApAp + blockIdx.x] = v[1];
+    }
+  } else if (RED == 3) {
     // per-block partial of Re <xs, out>, added up by the next kernel
     __shared__ double sh3[32];
     double v[1] = {dot};
@@ -599,6 +698,7 @@ static int launch_lo(const DslashArgsLo &A, int) {
 //   which 0: t = (2D)_{q,par} p                (out: PREC, hop +1)
 //   which 1: ap = 4 m2 p - (2D)_{par,q} t      (out: FP32, hop -1, pAp)
 //   red 3: per-block partials of <p, Ap> in partials[0 .. *blocks)
+//   red 4: those and per-block partials of |Ap|^2 from partials[kMxApAp]
 template <int PREC, int NL>
 static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int *blocks) {
   constexpr int VP = VecPrec<PREC>::v;
@@ -611,6 +711,8 @@ static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int 
     used = launch_lo<PREC, VP, NL, -1, 1, 2, kF32>(A, grid);
   } else if (red == 3) {
     used = launch_lo<PREC, VP, NL, -1, 1, 3, kF32>(A, grid);
+  } else if (red == 4) {
+    used = launch_lo<PREC, VP, NL, -1, 1, 4, kF32>(A, grid);
   } else {
     used = launch_lo<PREC, VP, NL, -1, 1, 0, kF32>(A, grid);
   }
@@ -811,59 +913,129 @@ __global__ void __launch_bounds__(kBlock)
   if (threadIdx.x == 0) r2p[blockIdx.x] = v[0];
 }
 
-// |r|^2 from the update's np per-block partials at r2p (added in the same
-// order by every block), the reliable-update test (|r| against delta times
-// the largest |r| since the last update), then p = r + beta p unless an
-// update is due.  Block 0 records the state.  The fields other blocks read are not written
-// here (r0Norm, delta, r2stop, itn, r2old) or are maxima that come out the
-// same whether read before or after block 0's write (maxrr, maxrx).
+// The fused update of the three-kernel iteration (iteration k + 1):
+//   the reliable-update test of |r_{k+1}|^2 (the previous update's per-block
+//   partials at r2in, nr2 of them; nr2 = 0 right after the start or a
+//   reliable update, when r2 is the state's), then
+//   rs -= alpha ap; xs += alpha p_in; p_out = rs + beta p_in
+// with alpha = r2 / <p, Ap> and beta = (alpha^2 |Ap|^2 - r2) / r2 from the
+// half sweep's per-block partials (np of each).  Every block adds each set
+// of partials in the same order, so all take the same decisions.  beta is
+// CG's |r_new|^2 / |r|^2 through |r - alpha Ap|^2 = r2 - 2 alpha <r, Ap> +
+// alpha^2 |Ap|^2 with <r, Ap> = <p, Ap> (p is A-orthogonal to the previous
+// direction), so p needs no second pass over the sites; the exact
+// |r_new|^2 is summed as well (per-block partials at r2out) for the next
+// update's alpha and test.  When the test stops the iteration nothing is
+// written: p_in, the direction a reliable update corrects, is intact in its
+// buffer (p_out is the other one), and the half sweeps of this iteration
+// were spent for nothing (once per reliable update).  Block 0 records the
+// state; the iteration count the blocks test is itc[par], and block 0 writes
+// itc[par ^ 1] (the host alternates par; a reliable update sets both).
+template <int PREC>
+__global__ void __launch_bounds__(kBlock)
+    mx_update_p_kernel(float2 *__restrict__ rs, float2 *__restrict__ xs, const float2 *__restrict__ ap,
+                       const void *pin, void *pout, int n, MxState *st, const double *pap, const double *apap,
+                       int np, const double *r2in, int nr2, double *r2out, int par) {
+  pdl_wait();
+  if (mx_halt(st)) return;
+  // the first site's operands are loaded before the sums of the partials,
+  // so that their latencies overlap
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  float2 pv[3], rv[3], av[3], xv[3];
+  if (i0 < n) {
+    load_vec<PREC>(pin, n, i0, pv);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      rv[c] = rs[(size_t)c * n + i0];
+      av[c] = ap[(size_t)c * n + i0];
+      xv[c] = xs[(size_t)c * n + i0];
+    }
+  }
+  // the partials, summed by the whole block (one round of loads)
+  __shared__ float sh_ab[2];
+  __shared__ int sh_go;
+  {
+    double v3[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+      v3[0] += __ldcg(pap + i);
+      v3[1] += __ldcg(apap + i);
+    }
+    for (int i = threadIdx.x; i < nr2; i += blockDim.x) v3[2] += __ldcg(r2in + i);
+    __shared__ double shp[96];
+    block_sum<3>(v3, shp);
+    if (threadIdx.x == 0) {
+      const double s = v3[0], q = v3[1];
+      const int itn = st->itc[par];
+      double r2 = st->r2;
+      bool go = true;
+      if (nr2 > 0) {
+        r2 = v3[2];
+        go = mx_test(st, r2, itn);
+      }
+      if (go) {
+        const double alpha = r2 / s;
+        const double beta = (alpha * alpha * q - r2) / r2;
+        sh_ab[0] = (float)alpha;
+        sh_ab[1] = (float)beta;
+        if (blockIdx.x == 0) {
+          st->pAp = s;
+          st->alpha = alpha;
+          st->beta = beta;
+          st->itn = itn + 1;
+          st->itc[par ^ 1] = itn + 1;
+          st->r2old = r2;
+          st->pin = par;
+        }
+      }
+      sh_go = go ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  if (!sh_go) return;
+  const float alpha = sh_ab[0], beta = sh_ab[1];
+  double s = 0.0;
+  for (int i = i0; i < n; i += gridDim.x * blockDim.x) {
+    if (i != i0) {
+      load_vec<PREC>(pin, n, i, pv);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        rv[c] = rs[(size_t)c * n + i];
+        av[c] = ap[(size_t)c * n + i];
+        xv[c] = xs[(size_t)c * n + i];
+      }
+    }
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float2 r = rv[c], x = xv[c];
+      r.x = fmaf(-alpha, av[c].x, r.x);
+      r.y = fmaf(-alpha, av[c].y, r.y);
+      x.x = fmaf(alpha, pv[c].x, x.x);
+      x.y = fmaf(alpha, pv[c].y, x.y);
+      rs[(size_t)c * n + i] = r;
+      xs[(size_t)c * n + i] = x;
+      acc = fmaf(r.x, r.x, acc);
+      acc = fmaf(r.y, r.y, acc);
+      pv[c] = make_float2(fmaf(beta, pv[c].x, r.x), fmaf(beta, pv[c].y, r.y));
+    }
+    store_vec<PREC>(pout, n, i, pv);
+    s += (double)acc;
+  }
+  __shared__ double sh[32];
+  double v[1] = {s};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) r2out[blockIdx.x] = v[0];
+}
+
+// |r|^2 and the reliable-update test (mx_decide), then p = r + beta p unless
+// an update is due (the four-kernel iteration of the domain solve).
 template <int PREC>
 __global__ void mx_p_kernel(const float2 *__restrict__ rs, void *p, int n, MxState *st, const double *r2p,
                             int np) {
   pdl_wait();
   if (mx_halt(st)) return;
-  __shared__ float sh_beta;
-  __shared__ int sh_go;
-  if (threadIdx.x < 32) {
-    double r2 = 0.0;
-    for (int i = threadIdx.x; i < np; i += 32) r2 += __ldcg(r2p + i);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-    if (threadIdx.x == 0) {
-      int go = 0;
-      double beta = 0.0;
-      if (!isfinite(r2)) {
-        if (blockIdx.x == 0) {
-          st->r2 = r2;
-          st->nan = 1;
-          st->done = 1;
-        }
-      } else {
-        const double rn = sqrt(r2);
-        const double maxrr = fmax(st->maxrr, rn), maxrx = fmax(st->maxrx, rn);
-        const bool ux = rn < st->delta * st->r0Norm && st->r0Norm <= maxrx;
-        const bool ur = (rn < st->delta * maxrr && st->r0Norm <= maxrr) || ux;
-        const bool pend = ur || r2 <= st->r2stop || st->itn >= st->maxits;
-        beta = r2 / st->r2old;
-        go = pend ? 0 : 1;
-        if (blockIdx.x == 0) {
-          st->r2 = r2;
-          st->rNorm = rn;
-          st->maxrr = maxrr;
-          st->maxrx = maxrx;
-          if (pend)
-            st->pending = 1;
-          else
-            st->beta = beta;
-        }
-      }
-      sh_beta = (float)beta;
-      sh_go = go;
-    }
-  }
-  __syncthreads();
-  if (!sh_go) return;
-  const float beta = sh_beta;
+  float beta;
+  if (!mx_decide(st, r2p, np, &beta)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float2 pv[3];
     load_vec_cg<PREC>(p, n, i, pv);
@@ -922,6 +1094,7 @@ __global__ void __launch_bounds__(kBlock)
     const double rn = sqrt(r2);
     st->rNorm = st->r0Norm = st->maxrr = st->maxrx = rn;
     st->beta = r2 / st->r2old;
+    st->itc[0] = st->itc[1] = st->itn;
   }
 }
 
@@ -982,14 +1155,17 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   Workspace &ws = g->ws;
   const size_t v64 = sizeof(double2) * 3 * (size_t)nh, v32 = sizeof(float2) * 3 * (size_t)nh;
   const size_t vp = (VP == kF32) ? v32 : sizeof(uint4) * (size_t)nh;
-  void *pr, *pax, *prs, *pxs, *pap, *pp, *pt, *pt64, *pst;
+  void *pr, *pax, *prs, *pxs, *pap, *pp, *pp2, *pt, *pt64, *pst;
   int rc;
   if ((rc = ws.get(kSlotMx0 + 0, v64, &pr)) || (rc = ws.get(kSlotMx0 + 1, v64, &pax)) ||
       (rc = ws.get(kSlotMx0 + 2, v32, &prs)) || (rc = ws.get(kSlotMx0 + 3, v32, &pxs)) ||
       (rc = ws.get(kSlotMx0 + 4, v32, &pap)) || (rc = ws.get(kSlotMx0 + 5 + 2 * VP, vp, &pp)) ||
       (rc = ws.get(kSlotMx0 + 6 + 2 * VP, vp, &pt)) || (rc = ws.get(kSlotMx0 + 9, v64, &pt64)) ||
-      (rc = ws.get(kSlotMx0 + 10, sizeof(MxState), &pst)))
+      (rc = ws.get(kSlotMx0 + 10, sizeof(MxState), &pst)) || (rc = ws.get(kSlotMx0 + 12 + VP, vp, &pp2)))
     return rc;
+  // p alternates between two buffers: each fused update reads one and
+  // writes the other
+  void *const P[2] = {pp, pp2};
   double2 *r = (double2 *)pr, *ax = (double2 *)pax;
   float2 *rs = (float2 *)prs, *xs = (float2 *)pxs, *ap = (float2 *)pap;
   MxState *st = (MxState *)pst;
@@ -1010,19 +1186,25 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   note_launch();
   QS_LAUNCH_CHECK();
   const int every = check_interval(nh);
+  // Three kernels an iteration: the two half sweeps (the second leaves the
+  // <p, Ap> and |Ap|^2 partials) and the fused update, which first tests the
+  // previous update's |r|^2 (except right after the start or a reliable
+  // update).  cur: the host parity of the next iteration, which reads p from
+  // P[cur] and |r|^2 partials from R2[cur], and writes P[cur ^ 1], R2[cur ^ 1].
+  int cur = 0;
+  bool fresh = true;
+  double *const R2[2] = {red_partials() + kMxR2, red_partials() + kMxR2b};
   auto batch = [&]() -> int {
     for (int i = 0; i < every; i++) {
       int np = 0;
-      int rc2 = schur_lo(g, PREC, par, ap, pp, pt, m2, 3, st, st, nullptr, &np);
+      int rc2 = schur_lo(g, PREC, par, ap, P[cur], pt, m2, 4, st, st, nullptr, &np);
       if (rc2) return rc2;
-      // <p, Ap> partials in the first kMaxRedBlocks doubles of the scratch,
-      // the update's |r|^2 partials after them; each summed by the next kernel
-      double *r2p = red_partials() + kMaxRedBlocks;
-      launch_pdl(mx_update_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)pp, nh, st,
-                 (const double *)red_partials(), np, r2p);
-      launch_pdl(mx_p_kernel<VP>, egrid, kBlock, (const float2 *)rs, (void *)pp, nh, st, (const double *)r2p,
-                 grid);
-      note_launch(2);
+      launch_pdl(mx_update_p_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)P[cur],
+                 P[cur ^ 1], nh, st, (const double *)red_partials(), (const double *)(red_partials() + kMxApAp),
+                 np, (const double *)R2[cur], fresh ? 0 : grid, R2[cur ^ 1], cur);
+      note_launch();
+      cur ^= 1;
+      fresh = false;
     }
     QS_LAUNCH_CHECK();
     return QEXSTAG_OK;
@@ -1038,14 +1220,19 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
       return rc;
     if (hs.done) break;
     if (!hs.pending) continue;
-    // reliable update: fold the increment in, FP64 true residual
+    // reliable update: fold the increment in, FP64 true residual; the
+    // direction corrected is the one the last update that ran read
+    // (P[hs.pin]: the update that stopped wrote nothing, and the kernels
+    // queued after it returned at once), and the iteration goes on from it
     mx_flush_kernel<<<egrid, kBlock, 0, stream()>>>(x.p, xs, nh);
     note_launch();
     if ((rc = schur64(g, par, VecD{ax, nh}, cv(x), VecD{(double2 *)pt64, nh}, m2))) return rc;
+    cur = hs.pin & 1;
+    fresh = true;
     mx_true_res_kernel<<<grid, kBlock, 0, stream()>>>(b.p, b.stride, ax, r, rs, nh, st, red_partials(),
                                                       red_tickets());
-    mx_rp_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, pp, nh, st, red_partials(), red_tickets());
-    mx_p_reliable_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, pp, nh, st);
+    mx_rp_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, P[cur], nh, st, red_partials(), red_tickets());
+    mx_p_reliable_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, P[cur], nh, st);
     mx_clear_pending_kernel<<<1, 1, 0, stream()>>>(st);
     note_launch(4);
     QS_LAUNCH_CHECK();

@@ -176,6 +176,11 @@ class DomainSet:
             out[ix] = p
         return out
 
+    @property
+    def recon12(self) -> bool:
+        """True when every domain keeps 12-real reduced-precision long links."""
+        return all(self.lib.qexstag_domain_recon12(h) == 1 for h in self.handles)
+
     def set_links(self, g: np.ndarray) -> None:
         self._links = self.split_links(np.ascontiguousarray(g, dtype=np.complex128))
         L.check(self.lib.qexstag_domain_links(self._set(), len(self.handles),

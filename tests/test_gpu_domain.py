@@ -34,6 +34,9 @@ def test_schur_matches_single_lattice(cuda, dims, nl, ranks):
     for R in ranks:
         d = DD.DomainSet(dims, R, nl)
         d.set_links(g)
+        # every slab's long links pass the 12-real check against signs
+        # rebuilt from global time
+        assert d.recon12 == (nl == 8), R
         r = x.copy()
         d.stagD2ee(r, x, 0.04)
         # even sites bit-exact (the same kernels, the same order per site);
@@ -146,6 +149,7 @@ def test_zt_schur_matches_single_lattice(cuda, dims, nl, grids):
         d = DD.DomainSet(dims, Rz * Rt, nl, grid=(Rz, Rt))
         assert d.ldims == (dims[0], dims[1], dims[2] // Rz, dims[3] // Rt)
         d.set_links(g)
+        assert d.recon12 == (nl == 8), (Rz, Rt)
         r = x.copy()
         d.stagD2ee(r, x, 0.04)
         assert np.array_equal(r[: V // 2], ref[: V // 2]), (Rz, Rt)

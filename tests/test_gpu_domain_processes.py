@@ -56,7 +56,7 @@ def _worker(rank, world, port, q, dims, grid):
             d.solveEE(y16, b, M, sp16)
         ix = d.gidx[0]
         q.put((rank, ix, r[ix], y[ix], sp.iterations, sp.r2, sp.status, y16[ix], sp16.r2, sp16.status,
-               sp16.reliable_updates))
+               sp16.reliable_updates, d.recon12))
         del d
     finally:
         dist.destroy_process_group()
@@ -85,11 +85,14 @@ def test_two_process_domain_solve(cuda, dims, grid):
     r = np.zeros_like(x)
     y = np.zeros_like(b)
     y16 = np.zeros_like(b)
-    for rank, ix, rp, yp, its, r2, status, y16p, r216, st16, rel16 in out:
+    for rank, ix, rp, yp, its, r2, status, y16p, r216, st16, rel16, rc12 in out:
         r[ix] = rp
         y[ix] = yp
         y16[ix] = y16p
         assert status == 0 and r2 <= 1e-20
+        # each slab's long links carry the global time boundary, so the
+        # 16-bit links keep 12 reals on both ranks
+        assert rc12
         if grid is None:
             assert st16 == 0 and r216 <= 1e-20 and rel16 >= 1
     # the Schur operator: bit for bit the single-lattice one
@@ -127,6 +130,9 @@ def test_one_domain_mixed_solve(cuda, dims):
     b = F.even_source(dims, 24)
     d = DD.DomainSet(dims, 1, 8)
     d.set_links(g)
+    # the ghost slices wrap around the antiperiodic boundary: the long-link
+    # signs rebuilt from global time match, and 12 reals are kept
+    assert d.recon12
     y = np.zeros_like(b)
     sp = S.SolverParams(r2req=1e-20, sloppySolve=S.L.SLOPPY_HALF, delta=0.1)
     d.solveEE(y, b, M, sp)
