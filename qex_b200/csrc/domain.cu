@@ -760,20 +760,21 @@ static int mx_exchange_even(void *ctx, void *field) {
   return exchange(&d, 1, &f, 1, 0, stream());
 }
 
-static int mx_allreduce(void *ctx, double *dev) {
+static int mx_allreduce(void *ctx, double *dev, int n) {
   qexstag_domain_s *d = ((MixedCtx *)ctx)->d;
   if (d->hostc) {
     double *h = host_results();
-    QS_CUDA(cudaMemcpyAsync(h, dev, sizeof(double), cudaMemcpyDeviceToHost, stream()));
+    QS_CUDA(cudaMemcpyAsync(h, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, stream()));
     QS_CUDA(cudaStreamSynchronize(stream()));
-    double v = h[0];
-    if (d->hc.all_reduce_sum(d->hc.ctx, &v, 1))
+    double v[4];
+    std::memcpy(v, h, sizeof(double) * n);
+    if (d->hc.all_reduce_sum(d->hc.ctx, v, n))
       return fail(QEXSTAG_ERR_STATE, "domain: the host communicator's sum reported an error");
-    h[0] = v;
-    QS_CUDA(cudaMemcpyAsync(dev, h, sizeof(double), cudaMemcpyHostToDevice, stream()));
+    std::memcpy(h, v, sizeof(double) * n);
+    QS_CUDA(cudaMemcpyAsync(dev, h, sizeof(double) * n, cudaMemcpyHostToDevice, stream()));
     QS_CUDA(cudaStreamSynchronize(stream()));  // h is reused by the next call
   } else if (d->comm) {
-    QS_NCCL(nccl().allReduce(dev, dev, 1, ncclDouble, ncclSum, d->comm, stream()));
+    QS_NCCL(nccl().allReduce(dev, dev, n, ncclDouble, ncclSum, d->comm, stream()));
   }
   return QEXSTAG_OK;
 }

@@ -88,7 +88,7 @@ int dslash64(const qexstag_links_s *g, int po, VecD out, CVecD xin, CVecD xs, CV
 struct MxDomain {
   void *ctx;
   int (*exchange_even)(void *ctx, void *field);
-  int (*allreduce)(void *ctx, double *dev);
+  int (*allreduce)(void *ctx, double *dev, int n);  // n device doubles summed over the processes, in place
   int (*schur64)(void *ctx, const double2 *x, double2 *ax);
   qexstag_links_s *g;
   int even_lo, n, odd_lo, odd_hi;

@@ -311,31 +311,6 @@ __device__ __forceinline__ bool mx_test(MxState *st, double r2, int itn) {
   return !pend;
 }
 
-// |r|^2 from the update's np per-block partials at r2p (added in the same
-// order by every block), then mx_test; *beta_out = r2 / r2old (recorded by
-// block 0 when the iteration goes on).  itn and r2old are not written in
-// the kernels that call this.
-__device__ __forceinline__ bool mx_decide(MxState *st, const double *r2p, int np, float *beta_out) {
-  __shared__ float sh_beta;
-  __shared__ int sh_go;
-  if (threadIdx.x < 32) {
-    double r2 = 0.0;
-    for (int i = threadIdx.x; i < np; i += 32) r2 += __ldcg(r2p + i);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-    if (threadIdx.x == 0) {
-      const bool go = mx_test(st, r2, st->itn);
-      const double beta = go ? r2 / st->r2old : 0.0;
-      if (go && blockIdx.x == 0) st->beta = beta;
-      sh_beta = (float)beta;
-      sh_go = go ? 1 : 0;
-    }
-  }
-  __syncthreads();
-  if (beta_out) *beta_out = sh_beta;
-  return sh_go != 0;
-}
-
 // ---------------------------------------------------------------------------
 // sloppy Dslash: out = b*xs + hop * sum_k [...]; fat and long partial sums
 // are kept apart so that the FP16 list scales multiply them once per site.
@@ -372,7 +347,6 @@ struct DslashArgsLo {
   int ostride;
   float b;
   const MxState *halt;  // stop when done or pending (may be null)
-  MxState *state;       // pAp finalisation (RED == 1)
   double *partials;
   unsigned *ticket;
   double *dot_out;      // RED == 2
@@ -489,23 +463,9 @@ __global__ void __launch_bounds__(kBlock, PREC == kF16 ? 4 : 1) dslash_lo_kernel
       A.partials[blockIdx.x] = v[0];
       A.partials[kMxApAp + blockIdx.x] = v[1];
     }
-  } else if (RED == 3) {
-    __shared__ double sh3[32];
-    double v[1] = {dot};
-    block_sum<1>(v, sh3);
-    if (threadIdx.x == 0) A.partials[blockIdx.x] = v[0];
-  } else if (RED) {
+  } else if (RED == 2) {
     double v[1] = {dot}, s[1];
-    if (grid_reduce<1>(v, A.partials, A.ticket, s) && threadIdx.x == 0) {
-      if (RED == 1) {
-        MxState *st = A.state;
-        st->pAp = s[0];
-        st->alpha = st->r2 / s[0];
-        st->itn += 1;
-      } else {
-        *A.dot_out = s[0];
-      }
-    }
+    if (grid_reduce<1>(v, A.partials, A.ticket, s) && threadIdx.x == 0) *A.dot_out = s[0];
   }
 }
 
@@ -620,24 +580,9 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
       A.partials[blockIdx.x] = v[0];
       A.partials[kMxApAp + blockIdx.x] = v[1];
     }
-  } else if (RED == 3) {
-    // per-block partial of Re <xs, out>, added up by the next kernel
-    __shared__ double sh3[32];
-    double v[1] = {dot};
-    block_sum<1>(v, sh3);
-    if (threadIdx.x == 0) A.partials[blockIdx.x] = v[0];
-  } else if (RED) {
+  } else if (RED == 2) {
     double v[1] = {dot}, sm[1];
-    if (grid_reduce<1>(v, A.partials, A.ticket, sm) && threadIdx.x == 0) {
-      if (RED == 1) {
-        MxState *st = A.state;
-        st->pAp = sm[0];
-        st->alpha = st->r2 / sm[0];
-        st->itn += 1;
-      } else {
-        *A.dot_out = sm[0];
-      }
-    }
+    if (grid_reduce<1>(v, A.partials, A.ticket, sm) && threadIdx.x == 0) *A.dot_out = sm[0];
   }
 }
 
@@ -697,20 +642,17 @@ static int launch_lo(const DslashArgsLo &A, int) {
 // the two half sweeps of the sloppy Schur operator:
 //   which 0: t = (2D)_{q,par} p                (out: PREC, hop +1)
 //   which 1: ap = 4 m2 p - (2D)_{par,q} t      (out: FP32, hop -1, pAp)
-//   red 3: per-block partials of <p, Ap> in partials[0 .. *blocks)
-//   red 4: those and per-block partials of |Ap|^2 from partials[kMxApAp]
+//   red 2: Re <p, Ap> summed into *dot_out (last-block reduction)
+//   red 4: per-block partials of <p, Ap> in partials[0 .. *blocks) and of
+//          |Ap|^2 from partials[kMxApAp]
 template <int PREC, int NL>
 static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int *blocks) {
   constexpr int VP = VecPrec<PREC>::v;
   int used;
   if (which == 0) {
     used = launch_lo<PREC, VP, NL, 1, 0, 0, VP>(A, grid);
-  } else if (red == 1) {
-    used = launch_lo<PREC, VP, NL, -1, 1, 1, kF32>(A, grid);
   } else if (red == 2) {
     used = launch_lo<PREC, VP, NL, -1, 1, 2, kF32>(A, grid);
-  } else if (red == 3) {
-    used = launch_lo<PREC, VP, NL, -1, 1, 3, kF32>(A, grid);
   } else if (red == 4) {
     used = launch_lo<PREC, VP, NL, -1, 1, 4, kF32>(A, grid);
   } else {
@@ -724,13 +666,12 @@ static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int 
 // sloppy Schur: ap (FP32 [3][nh]) = 4 m2 p - (2D)(2D) p on parity par,
 // p and t in format prec.
 int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void *p, void *t,
-             double m2, int red, MxState *state, const MxState *halt, double *dot_out, int *red_blocks) {
+             double m2, int red, const MxState *halt, double *dot_out, int *red_blocks) {
   const Geom &geo = g->l->g;
   DslashArgsLo A;
   A.g = geo;
   A.L = lo_links(g->low, prec);
   A.halt = halt;
-  A.state = state;
   A.partials = red_partials();
   A.ticket = red_tickets();
   A.dot_out = dot_out;
@@ -776,7 +717,6 @@ int schur_lo_v32(const qexstag_links_s *g, int prec, int par, float2 *ap, const 
   A.g = geo;
   A.L = lo_links(g->low, prec);
   A.halt = nullptr;
-  A.state = nullptr;
   A.partials = red_partials();
   A.ticket = red_tickets();
   A.dot_out = dot_out;
@@ -852,65 +792,6 @@ __global__ void __launch_bounds__(kBlock)
     st->nan = isfinite(b2) ? 0 : 1;
     st->done = (!(b2 > st->r2stop) || st->maxits <= 0 || st->nan) ? 1 : 0;
   }
-}
-
-// alpha = r2 / pAp from the np per-block partials of <p, Ap> the half sweep
-// left (cg.nim:213-215): every block adds them in the same order, so all
-// get the same alpha; block 0 records pAp, alpha and the iteration
-__device__ __forceinline__ float mx_alpha(const double *pap, int np, MxState *st) {
-  __shared__ double sh_alpha;
-  if (threadIdx.x < 32) {
-    double s = 0.0;
-    for (int i = threadIdx.x; i < np; i += 32) s += __ldcg(pap + i);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) {
-      const double alpha = st->r2 / s;
-      sh_alpha = alpha;
-      if (blockIdx.x == 0) {
-        st->pAp = s;
-        st->alpha = alpha;
-        st->itn += 1;
-        st->r2old = st->r2;  // beta's denominator for mx_p_kernel
-      }
-    }
-  }
-  __syncthreads();
-  return (float)sh_alpha;
-}
-
-// rs -= alpha ap; xs += alpha p, with alpha from the half sweep's <p, Ap>
-// partials at pap (mx_alpha); |r|^2 per block into r2p[blockIdx.x]
-template <int PREC>
-__global__ void __launch_bounds__(kBlock)
-    mx_update_kernel(float2 *__restrict__ rs, float2 *__restrict__ xs, const float2 *__restrict__ ap,
-                     const void *p, int n, MxState *st, const double *pap, int np, double *r2p) {
-  pdl_wait();
-  if (mx_halt(st)) return;
-  const float alpha = mx_alpha(pap, np, st);
-  double s = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float2 pv[3];
-    load_vec<PREC>(p, n, i, pv);
-    float acc = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      float2 r = rs[(size_t)c * n + i], a = ap[(size_t)c * n + i], xv = xs[(size_t)c * n + i];
-      r.x = fmaf(-alpha, a.x, r.x);
-      r.y = fmaf(-alpha, a.y, r.y);
-      xv.x = fmaf(alpha, pv[c].x, xv.x);
-      xv.y = fmaf(alpha, pv[c].y, xv.y);
-      rs[(size_t)c * n + i] = r;
-      xs[(size_t)c * n + i] = xv;
-      acc = fmaf(r.x, r.x, acc);
-      acc = fmaf(r.y, r.y, acc);
-    }
-    s += (double)acc;
-  }
-  __shared__ double sh[32];
-  double v[1] = {s};
-  block_sum<1>(v, sh);
-  if (threadIdx.x == 0) r2p[blockIdx.x] = v[0];
 }
 
 // The fused update of the three-kernel iteration (iteration k + 1):
@@ -1025,27 +906,6 @@ __global__ void __launch_bounds__(kBlock)
   double v[1] = {s};
   block_sum<1>(v, sh);
   if (threadIdx.x == 0) r2out[blockIdx.x] = v[0];
-}
-
-// |r|^2 and the reliable-update test (mx_decide), then p = r + beta p unless
-// an update is due (the four-kernel iteration of the domain solve).
-template <int PREC>
-__global__ void mx_p_kernel(const float2 *__restrict__ rs, void *p, int n, MxState *st, const double *r2p,
-                            int np) {
-  pdl_wait();
-  if (mx_halt(st)) return;
-  float beta;
-  if (!mx_decide(st, r2p, np, &beta)) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float2 pv[3];
-    load_vec_cg<PREC>(p, n, i, pv);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      float2 r = rs[(size_t)c * n + i];
-      pv[c] = make_float2(fmaf(beta, pv[c].x, r.x), fmaf(beta, pv[c].y, r.y));
-    }
-    store_vec<PREC>(p, n, i, pv);
-  }
 }
 
 // reliable update part 1: x += xs, xs = 0
@@ -1197,7 +1057,7 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   auto batch = [&]() -> int {
     for (int i = 0; i < every; i++) {
       int np = 0;
-      int rc2 = schur_lo(g, PREC, par, ap, P[cur], pt, m2, 4, st, st, nullptr, &np);
+      int rc2 = schur_lo(g, PREC, par, ap, P[cur], pt, m2, 4, st, nullptr, &np);
       if (rc2) return rc2;
       launch_pdl(mx_update_p_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)P[cur],
                  P[cur ^ 1], nh, st, (const double *)red_partials(), (const double *)(red_partials() + kMxApAp),
@@ -1270,9 +1130,10 @@ int cg_mixed(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, double r2r
 // sweep 1 on the odd slices the second needs ([odd_lo, odd_hi), reaching
 // rho slices into the ghosts), half sweep 2 and the vector updates on the
 // interior even sites.  Before half sweep 1 the ghost slices of p (16 bytes
-// per site) are exchanged, and every sum (<p, Ap>, |r|^2, and at reliable
-// updates |b - Ax|^2 and <r, p>) is the domain's partial, added in block
-// order, then summed over the processes, before the state kernels use it.
+// per site) are exchanged, and every sum (<p, Ap>, |Ap|^2 and |r|^2 once per
+// iteration, and at reliable updates |b - Ax|^2 and <r, p>) is the domain's
+// partial, added in block order, then summed over the processes, before the
+// state kernels use it.
 // The caller provides the exchange, the sum and the FP64 Schur operator of
 // the decomposed lattice (MxDomain).
 // ---------------------------------------------------------------------------
@@ -1284,6 +1145,26 @@ __global__ void mxd_sum_kernel(const double *partials, int np, double *val) {
   for (int i = threadIdx.x; i < np; i += blockDim.x) v[0] += __ldcg(partials + i);
   block_sum<1>(v, sh);
   if (threadIdx.x == 0) *val = v[0];
+}
+
+// the three sums of an iteration, in block order: <p, Ap> and |Ap|^2 (np
+// half-sweep partials each) and the previous update's |r|^2 (nr2 partials,
+// 0 when there is none) into val[0..2]
+__global__ void mxd_sum3_kernel(const double *pap, const double *apap, int np, const double *r2p, int nr2,
+                                double *val) {
+  __shared__ double sh[96];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    v[0] += __ldcg(pap + i);
+    v[1] += __ldcg(apap + i);
+  }
+  for (int i = threadIdx.x; i < nr2; i += blockDim.x) v[2] += __ldcg(r2p + i);
+  block_sum<3>(v, sh);
+  if (threadIdx.x == 0) {
+    val[0] = v[0];
+    val[1] = v[1];
+    val[2] = v[2];
+  }
 }
 
 // r = b, x = 0, rs = b, xs = 0, p = b; per-block |b|^2
@@ -1322,6 +1203,7 @@ __global__ void mxd_init_state_kernel(MxState *st, const double *b2p) {
   st->r2stop = st->r2req * b2;
   st->rNorm = st->r0Norm = st->maxrx = st->maxrr = sqrt(b2);
   st->itn = 0;
+  st->itc[0] = st->itc[1] = 0;
   st->pending = 0;
   st->reliable = 0;
   st->nan = isfinite(b2) ? 0 : 1;
@@ -1367,6 +1249,7 @@ __global__ void mxd_true_res_state_kernel(MxState *st, const double *r2p) {
   const double rn = sqrt(r2);
   st->rNorm = st->r0Norm = st->maxrr = st->maxrx = rn;
   st->beta = r2 / st->r2old;
+  st->itc[0] = st->itc[1] = st->itn;
 }
 
 // per-block <rs, p> (mx_rp_kernel without the grid reduction)
@@ -1407,23 +1290,30 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
   const int n = D.n, nh = geo.nh;
   Workspace &ws = g->ws;
   const size_t v64 = sizeof(double2) * 3 * (size_t)n, v32 = sizeof(float2) * 3 * (size_t)n;
-  void *pr, *pax, *prs, *pxs, *pap, *pp, *pt, *pst, *pval, *ppart;
+  void *pr, *pax, *prs, *pxs, *pap, *pp, *pp2, *pt, *pst, *pval, *ppart;
   int rc;
   if ((rc = ws.get(kSlotMx0 + 30, v64, &pr)) || (rc = ws.get(kSlotMx0 + 31, v64, &pax)) ||
       (rc = ws.get(kSlotMx0 + 32, v32, &prs)) || (rc = ws.get(kSlotMx0 + 33, v32, &pxs)) ||
       (rc = ws.get(kSlotMx0 + 34, v32, &pap)) || (rc = ws.get(kSlotMx0 + 35, sizeof(uint4) * (size_t)nh, &pp)) ||
       (rc = ws.get(kSlotMx0 + 36, sizeof(uint4) * (size_t)nh, &pt)) ||
       (rc = ws.get(kSlotMx0 + 37, sizeof(MxState), &pst)) || (rc = ws.get(kSlotMx0 + 38, sizeof(double) * 4, &pval)) ||
-      (rc = ws.get(kSlotMx0 + 39, sizeof(double) * 2 * kMaxRedBlocks, &ppart)))
+      (rc = ws.get(kSlotMx0 + 39, sizeof(double) * 4 * kMaxRedBlocks, &ppart)) ||
+      (rc = ws.get(kSlotMx0 + 40, sizeof(uint4) * (size_t)nh, &pp2)))
     return rc;
   double2 *r = (double2 *)pr, *ax = (double2 *)pax;
   float2 *rs = (float2 *)prs, *xs = (float2 *)pxs, *ap = (float2 *)pap;
-  uint4 *p = (uint4 *)pp, *t = (uint4 *)pt;
-  uint4 *pin = p + D.even_lo;  // the interior part of p, compact
+  uint4 *t = (uint4 *)pt;
+  // p alternates between two extended-lattice buffers (the fused update
+  // reads one and writes the other); PI: their interior parts, compact
+  uint4 *const P[2] = {(uint4 *)pp, (uint4 *)pp2};
+  uint4 *const PI[2] = {P[0] + D.even_lo, P[1] + D.even_lo};
   MxState *st = (MxState *)pst;
-  double *val = (double *)pval, *part = (double *)ppart, *part2 = part + kMaxRedBlocks;
+  // partials laid out as red_partials in cg_mixed_t
+  double *val = (double *)pval, *part = (double *)ppart;
+  double *const R2[2] = {part + kMxR2, part + kMxR2b};
   // zero p and t so that sites no sweep writes hold finite values
-  QS_CUDA(cudaMemsetAsync(p, 0, sizeof(uint4) * (size_t)nh, stream()));
+  QS_CUDA(cudaMemsetAsync(P[0], 0, sizeof(uint4) * (size_t)nh, stream()));
+  QS_CUDA(cudaMemsetAsync(P[1], 0, sizeof(uint4) * (size_t)nh, stream()));
   QS_CUDA(cudaMemsetAsync(t, 0, sizeof(uint4) * (size_t)nh, stream()));
   MxState hs;
   std::memset(&hs, 0, sizeof(hs));
@@ -1443,9 +1333,9 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
     mxd_sum_kernel<<<1, kBlock, 0, stream()>>>(partials, np, val);
     note_launch();
     QS_LAUNCH_CHECK();
-    return D.allreduce(D.ctx, val);
+    return D.allreduce(D.ctx, val, 1);
   };
-  mxd_init_kernel<VP><<<grid, kBlock, 0, stream()>>>(b, x, r, rs, xs, pin, n, part);
+  mxd_init_kernel<VP><<<grid, kBlock, 0, stream()>>>(b, x, r, rs, xs, PI[0], n, part);
   note_launch();
   QS_LAUNCH_CHECK();
   if ((rc = sum_over(part, grid))) return rc;
@@ -1455,12 +1345,11 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
   A1.g = geo;
   A1.L = lo_links(g->low, PREC);
   A1.halt = st;
-  A1.state = st;
   A1.partials = part;
   A1.ticket = red_tickets();
   A1.dot_out = nullptr;
   A1.po = 1;
-  A1.xin = p;
+  A1.xin = P[0];
   A1.istride = nh;
   A1.xs = nullptr;
   A1.sstride = 0;
@@ -1472,7 +1361,7 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
   A2 = A1;
   A2.po = 0;
   A2.xin = t;
-  A2.xs = p;
+  A2.xs = P[0];
   A2.sstride = nh;
   A2.out = ap;
   A2.ostride = n;
@@ -1480,38 +1369,53 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
   A2.b = (float)(4.0 * m2);
   A2.k_lo = D.even_lo;
   A2.k_hi = D.even_lo + n;
+  // The three-kernel iteration of cg_mixed_t with one sum over the
+  // processes per iteration: the ghost exchange of P[cur], the half sweeps,
+  // then <p, Ap>, |Ap|^2 and the previous update's |r|^2 summed in the
+  // domain and over the processes together, then the fused update.
+  int cur = 0;
+  bool fresh = true;
   auto iteration = [&]() -> int {
-    int rc2 = D.exchange_even(D.ctx, p);
+    int rc2 = D.exchange_even(D.ctx, P[cur]);
     if (rc2) return rc2;
     int np = 0;
+    A1.xin = P[cur];
+    A2.xs = P[cur];
     if ((rc2 = g->nl == 8 ? sloppy_half<PREC, 8>(0, A1, 0, 0, nullptr) : sloppy_half<PREC, 4>(0, A1, 0, 0, nullptr)))
       return rc2;
-    if ((rc2 = g->nl == 8 ? sloppy_half<PREC, 8>(1, A2, 0, 3, &np) : sloppy_half<PREC, 4>(1, A2, 0, 3, &np)))
+    if ((rc2 = g->nl == 8 ? sloppy_half<PREC, 8>(1, A2, 0, 4, &np) : sloppy_half<PREC, 4>(1, A2, 0, 4, &np)))
       return rc2;
-    if ((rc2 = sum_over(part, np))) return rc2;
-    launch_pdl(mx_update_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)pin, n, st,
-               (const double *)val, 1, part2);
-    note_launch();
-    if ((rc2 = sum_over(part2, grid))) return rc2;
-    launch_pdl(mx_p_kernel<VP>, egrid, kBlock, (const float2 *)rs, (void *)pin, n, st, (const double *)val, 1);
+    mxd_sum3_kernel<<<1, kBlock, 0, stream()>>>(part, part + kMxApAp, np, R2[cur], fresh ? 0 : grid, val);
     note_launch();
     QS_LAUNCH_CHECK();
+    if ((rc2 = D.allreduce(D.ctx, val, 3))) return rc2;
+    launch_pdl(mx_update_p_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)PI[cur],
+               (void *)PI[cur ^ 1], n, st, (const double *)val, (const double *)(val + 1), 1,
+               (const double *)(val + 2), fresh ? 0 : 1, R2[cur ^ 1], cur);
+    note_launch();
+    QS_LAUNCH_CHECK();
+    cur ^= 1;
+    fresh = false;
     return QEXSTAG_OK;
   };
-  auto reliable_update = [&]() -> int {
+  // the direction corrected is the one the last update that ran read
+  // (PI[hs.pin]); the iteration goes on from it
+  auto reliable_update = [&](int pin) -> int {
     mx_flush_kernel<<<egrid, kBlock, 0, stream()>>>(x, xs, n);
     note_launch();
     int rc2 = D.schur64(D.ctx, x, ax);
     if (rc2) return rc2;
+    cur = pin & 1;
+    fresh = true;
     mxd_true_res_kernel<<<grid, kBlock, 0, stream()>>>(b, ax, r, rs, n, part);
     note_launch();
     if ((rc2 = sum_over(part, grid))) return rc2;
     mxd_true_res_state_kernel<<<1, 1, 0, stream()>>>(st, val);
-    mxd_rp_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, pin, n, part);
+    mxd_rp_kernel<VP><<<grid, kBlock, 0, stream()>>>(rs, PI[cur], n, part);
     note_launch(2);
     if ((rc2 = sum_over(part, grid))) return rc2;
     mxd_set_rp_kernel<<<1, 1, 0, stream()>>>(st, val);
-    mx_p_reliable_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, pin, n, st);
+    mx_p_reliable_kernel<VP><<<egrid, kBlock, 0, stream()>>>(rs, PI[cur], n, st);
     mx_clear_pending_kernel<<<1, 1, 0, stream()>>>(st);
     note_launch(3);
     QS_LAUNCH_CHECK();
@@ -1526,7 +1430,7 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
       if ((rc = iteration())) return rc;
     if ((rc = snap.start(st, sizeof(MxState))) || (rc = snap.wait(&hs, sizeof(MxState)))) return rc;
     if (hs.done) break;
-    if (hs.pending && (rc = reliable_update())) return rc;
+    if (hs.pending && (rc = reliable_update(hs.pin))) return rc;
   }
   out->iterations = hs.itn;
   out->r2 = hs.b2 > 0 ? hs.r2 / hs.b2 : 0.0;
@@ -1594,8 +1498,7 @@ int bench_schur(qexstag_links_s *g, int prec, int nrep, double m2, double *sec) 
   auto once = [&]() -> int {
     if (prec == 0)
       return schur64(g, 0, VecD{(double2 *)pc, nh}, CVecD{(const double2 *)pa, nh}, VecD{(double2 *)pb, nh}, m2);
-    return schur_lo(g, prec == 1 ? kF32 : kF16, 0, (float2 *)pc, pa, pb, m2, 0, nullptr, nullptr, nullptr,
-                    nullptr);
+    return schur_lo(g, prec == 1 ? kF32 : kF16, 0, (float2 *)pc, pa, pb, m2, 0, nullptr, nullptr, nullptr);
   };
   for (int i = 0; i < 2; i++)
     if ((rc = once())) return rc;
