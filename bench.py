@@ -10,6 +10,7 @@ solve through the C ABI with host (QEX-layout) buffers, copies included.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--dims 32,32,32,32]
+  python bench.py --rows    (every hot-path row beside the oracle on the host)
 
 With N > 1 (torchrun) the lattice grows with N: 32^3 x (32 N), split along
 t into one 32^4 slab per GPU and solved by the domain decomposition's
@@ -335,6 +336,144 @@ def time_stagdn(s, nh, torch, peak):
     return out
 
 
+def run_rows(args):
+    """--rows: each hot-path row of the library on one GPU (device-resident
+    inputs, CUDA events on the library's stream) beside the oracle's CPU
+    restatement of QEX's code for it, on this box's host threads, on the
+    same fields.  Where a whole CPU call takes minutes the CPU leg runs a
+    bounded sample and scales it, and says so.  One JSON line."""
+    import torch
+
+    from oracle import oracle as O
+    from qex_b200 import fields as F
+    from qex_b200 import md as MD
+    from qex_b200 import smear as SM
+    from qex_b200 import stag as S
+    from qex_b200.batched_bench import problem_set
+    from qex_b200.multishift_bench import shifts
+    S.init(0)
+    S.set_stream(torch.cuda.current_stream().cuda_stream)
+
+    def gpu(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / reps
+
+    def cpu(fn, reps=1):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        return min(ts), out
+
+    rows = {}
+    dims = (32, 32, 32, 32)
+    V = F.volume(dims)
+    g = F.fat_naik_links(dims, 21)
+    s = S.Staggered(S.Layout(dims), S.to_device_links(g))
+    o = O.Oracle(dims, g)
+    # A7: the FP64 Schur operator stagD2ee
+    x = F.gaussian_vector(V, 3)
+    r = x.copy()
+    tc, _ = cpu(lambda: o.stagD2ee(r, x, 1e-4), 3)
+    rows["A7 stagD2ee FP64, 32^4 fat+Naik"] = {"gpu_s": s.bench_schur(0, 20, 1e-4), "cpu_s": tc,
+                                              "gpu_16bit_s": s.bench_schur(2, 20, 1e-4)}
+    # A9: stagDN on 8 fields against 8 oracle stagD2 calls
+    xs = [F.gaussian_vector(V, 10 + j) for j in range(8)]
+    rs = [v.copy() for v in xs]
+    xd = [S.to_device_vector(v) for v in xs]
+    rd = [torch.zeros_like(v) for v in xd]
+    tg = gpu(lambda: s.stagDN(0, rd, xd, 0.1), 10)
+    tc, _ = cpu(lambda: [o.stagD2(0, rr, xx, 0.0, 0.1) for rr, xx in zip(rs, xs)], 2)
+    rows["A9 stagDN FP64, 8 fields, 32^4 fat+Naik"] = {"gpu_s": tg, "cpu_s": tc}
+    # A14: FP64 multi-shift CG, 12 shifts, one right-hand side
+    sig = shifts(12)
+    b = F.even_source(dims, 100)
+    bd = S.to_device_vector(b)
+    ys = [torch.zeros((3, V), dtype=torch.complex128, device="cuda") for _ in sig]
+    sp = S.SolverParams(r2req=R2REQ)
+    tg = gpu(lambda: s.cgm_ee(MASS, sig, [bd], [ys], sp), 1)
+    its_g = sp.iterations
+    xo = [o.vec() for _ in sig]
+    k = 100
+    tc, (its_c, _) = cpu(lambda: o.cgm(0, xo, sig, b, MASS * MASS, R2REQ, maxits=k))
+    rows["A14 multi-shift CG FP64, 12 shifts, 32^4"] = {
+        "gpu_s": tg, "gpu_iterations": its_g, "cpu_s": tc / max(its_c, 1) * its_g,
+        "cpu_sample": f"{its_c} oracle CG-M iterations ({tc:.2f} s), scaled to the GPU's {its_g}"}
+    del s, o, ys, xd, rd
+    torch.cuda.empty_cache()
+    # C3: 64 small lattices, one persistent launch against the oracle's CG per lattice
+    stags, bds, ms, probs = [], [], [], problem_set(64)
+    for pd, pg, pm, pb in probs:
+        stags.append(S.Staggered(S.Layout(pd), S.to_device_links(pg)))
+        bds.append(S.to_device_vector(pb))
+        ms.append(pm)
+    xds = [torch.zeros_like(v) for v in bds]
+    S.solve_batched(stags, xds, bds, ms, S.SolverParams(r2req=R2REQ))  # launch configuration
+    tg = gpu(lambda: S.solve_batched(stags, xds, bds, ms, S.SolverParams(r2req=R2REQ)), 3)
+    tcs = 0.0
+    for pd, pg, pm, pb in probs:
+        oo = O.Oracle(pd, pg)
+        y = oo.vec()
+        t, _ = cpu(lambda: oo.cg(0, y, pb, pm * pm, R2REQ))
+        tcs += t
+        del oo
+    rows["C3 64 lattices {8^4, 12^4, 16^4, 8^3x16} to 1e-10"] = {"gpu_s": tg, "cpu_s": tcs}
+    del stags, bds, xds
+    torch.cuda.empty_cache()
+    # A16: the fermion force at 16^4 (solve to 1e-26 and outer products)
+    d4 = (16, 16, 16, 16)
+    g4 = F.fat_naik_links(d4, 21)
+    phi = F.even_source(d4, 33)
+    gd4 = S.to_device_links(g4)
+    s4 = S.Staggered(S.Layout(d4), gd4)
+    fd = torch.zeros_like(gd4)
+    phid = S.to_device_vector(phi)
+    tg = gpu(lambda: s4.force(fd, phid, 0.05, S.SolverParams(r2req=1e-26)), 2)
+    o4 = O.Oracle(d4, g4)
+    fo = np.zeros_like(g4)
+    tc, _ = cpu(lambda: o4.force(fo, phi, 0.05, 1e-26))
+    rows["A16 fermion force, 16^4 fat+Naik, m 0.05"] = {"gpu_s": tg, "cpu_s": tc}
+    del s4, o4, fd, gd4
+    # F1: HISQ smearing and its chain rule; F4: gauge force, 32^4
+    gw = F.apply_phases(dims, F.gauge_warm(dims, 0.3, 17))
+    gwd = S.to_device_links(gw)
+    lay = S.Layout(dims)
+    sm = SM.Smear(lay)
+    coef = SM.newHISQ()
+    fl, ll = torch.empty_like(gwd), torch.empty_like(gwd)
+    tg = gpu(lambda: sm.smear(coef, gwd, fl, ll), 5)
+    tc, _ = cpu(lambda: O.hisq_smear(dims, gw))
+    rows["F1 HISQ smear, 32^4"] = {"gpu_s": tg, "cpu_s": tc}
+    rng = np.random.default_rng(5)
+    cf = rng.standard_normal(gw.shape) + 1j * rng.standard_normal(gw.shape)
+    cl = np.ascontiguousarray(cf[::-1])
+    cfd, cld = S.to_device_links(cf), S.to_device_links(cl)
+    dd = torch.empty_like(gwd)
+    tg = gpu(lambda: sm.smearDeriv(coef, gwd, cfd, cld, dd), 3)
+    tc, _ = cpu(lambda: O.hisq_deriv(dims, gw, cf, cl))
+    rows["F1 HISQ chain rule, 32^4"] = {"gpu_s": tg, "cpu_s": tc}
+    u = F.gauge_warm(dims, 0.3, 3)
+    ud = S.to_device_links(u)
+    f = torch.empty_like(ud)
+    for name, c1 in (("Wilson", 0.0), ("Symanzik", -1.0 / 12)):
+        ga = MD.GaugeAction(lay, 5.6, c1)
+        tg = gpu(lambda: ga.force(ud, f), 5)
+        tc, _ = cpu(lambda: O.gauge_force(dims, u, 5.6 * (1 - 8 * c1), 5.6 * c1))
+        rows[f"F4 gauge force {name}, 32^4"] = {"gpu_s": tg, "cpu_s": tc}
+    for v in rows.values():
+        v["cpu_over_gpu"] = v["cpu_s"] / v["gpu_s"]
+    print(json.dumps({"rows": rows, "cpu_threads": O.num_threads(), "cpu_kind": "port",
+                      "device": torch.cuda.get_device_name(0)}), flush=True)
+
+
 def run_domain(args, dims, ws, rank, local):
     """N > 1: one lattice of dims[0] x dims[1] x dims[2] x (dims[3] N) split
     along t into N slabs of dims, one per rank (weak scaling), solved by the
@@ -586,12 +725,17 @@ def main():
     ap.add_argument("--ref-maxits", type=int, default=100000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-multishift", action="store_true", help="skip the multi-shift comparison")
+    ap.add_argument("--rows", action="store_true",
+                    help="instead: every hot-path row on the GPU beside the oracle on the host threads")
     ap.add_argument("--transport", default="nccl", choices=["nccl", "host"],
                     help="N > 1: domain exchanges over NCCL, or through host memory over gloo")
     ap.add_argument("--replicas", action="store_true",
                     help="N > 1: one independent 32^4 solve per GPU instead of the domain split")
     args = ap.parse_args()
     dims = tuple(int(v) for v in args.dims.split(","))
+    if args.rows and args.impl == "ours":
+        run_rows(args)
+        return
     if args.impl == "reference":
         if args.ref_iters <= 0:
             args.ref_iters = FP64_ITERS_32 if dims == (32, 32, 32, 32) else 100 * max(1, args.steps)
