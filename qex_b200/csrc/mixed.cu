@@ -801,12 +801,13 @@ __global__ void __launch_bounds__(kBlock)
 //   rs -= alpha ap; xs += alpha p_in; p_out = rs + beta p_in
 // with alpha = r2 / <p, Ap> and beta = (alpha^2 |Ap|^2 - r2) / r2 from the
 // half sweep's per-block partials (np of each).  Every block adds each set
-// of partials in the same order, so all take the same decisions.  beta is
-// CG's |r_new|^2 / |r|^2 through |r - alpha Ap|^2 = r2 - 2 alpha <r, Ap> +
-// alpha^2 |Ap|^2 with <r, Ap> = <p, Ap> (p is A-orthogonal to the previous
-// direction), so p needs no second pass over the sites; the exact
-// |r_new|^2 is summed as well (per-block partials at r2out) for the next
-// update's alpha and test.  When the test stops the iteration nothing is
+// of partials in the same order, so all take the same decisions.  In exact
+// arithmetic beta is CG's |r_new|^2 / |r|^2 (cg.nim:229-236), through
+// |r - alpha Ap|^2 = r2 - 2 alpha <r, Ap> + alpha^2 |Ap|^2 and <r, Ap> =
+// <p, Ap>; it is also the beta that makes the next direction A-orthogonal
+// to p, -<r_new, Ap> / <p, Ap>, under the same identity.  So p needs no
+// second pass over the sites; the exact |r_new|^2 is summed as well
+// (per-block partials at r2out) for the next update's alpha and test.  When the test stops the iteration nothing is
 // written: p_in, the direction a reliable update corrects, is intact in its
 // buffer (p_out is the other one), and the half sweeps of this iteration
 // were spent for nothing (once per reliable update).  Block 0 records the
