@@ -266,10 +266,10 @@ def time_multishift(s, dims, torch):
     """The mixed-precision multi-shift solve on the workload's lattice and
     fields: one Gaussian right-hand side, 12 shifts log-spaced from 1e-4 to
     1 (A + sigma_k, A = stagD2ee(m^2)), true FP64 residual 1e-10 for every
-    shift; 16-bit links in the multi-shift iterations, then each shift
-    refined by the reliable-update CG.  Beside it, the same systems by FP64
-    multi-shift CG and by one plain FP64 CG per shift.  One warm-up and one
-    timed call each (CUDA events)."""
+    shift; the SLOPPY_HALF call: FP32 links in the multi-shift iterations,
+    then each shift refined by the 16-bit reliable-update CG.  Beside it,
+    the same systems by FP64 multi-shift CG and by one plain FP64 CG per
+    shift.  One warm-up and one timed call each (CUDA events)."""
     from qex_b200 import fields as F
     from qex_b200 import stag as S
     from qex_b200.multishift_bench import shifts

@@ -698,8 +698,12 @@ int cgm_ee(qexstag_links_s *g, double m, int nshift, const double *sigma, int nr
     }
     int its = 0;
     if (sloppy) {
-      rc = cgm_core(g, 0, m2, nshift, sg.data(), nr, bb, V, yy, V, 1.0, r2ms, maxits, true, true, &its,
-                    p->sloppy == QEXSTAG_SLOPPY_HALF ? kF16 : kF32);
+      // FP32 links for the multi-shift phase at either sloppy precision: the
+      // shifted solutions come out as accurate as the links they were
+      // iterated with (about 1e-7 relative with FP32 links, 1e-4 with 16-bit
+      // ones), and the per-shift refinement below, in the call's precision,
+      // then covers three decades instead of six
+      rc = cgm_core(g, 0, m2, nshift, sg.data(), nr, bb, V, yy, V, 1.0, r2ms, maxits, true, true, &its, kF32);
     } else {
       rc = 0;
       for (int j = 0; j < nr && !rc; j++) {
