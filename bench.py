@@ -250,11 +250,12 @@ def iteration_breakdown(res, k, nh, peak, solver):
     times: the solve's time per iteration against the Schur operator's time
     per call; the rest is the fused update of r, x and p (16-bit solve: r,
     Ap, x in FP32 and p in 16 bits read, r, x and the next p written, 152 B
-    per even site), the reliable updates spread over the iterations, and
-    the kernel boundaries."""
+    per even site, and half sweep 2's read of r for <r, Ap>, 24 B), the
+    reliable updates spread over the iterations, and the kernel
+    boundaries."""
     it = res["time_s"] / max(res["iterations"], 1)
     rest = it - k["seconds"]
-    vec_bytes = {"fp16+fp64": 3 * 24 + 16 + 2 * 24 + 16, "fp32+fp64": 4 * 24 + 3 * 24,
+    vec_bytes = {"fp16+fp64": 3 * 24 + 16 + 2 * 24 + 16 + 24, "fp32+fp64": 4 * 24 + 3 * 24,
                  "fp64": 240 + 48 * 4}[solver]
     return {"us_per_iteration": round(it * 1e6, 2), "schur_us": round(k["seconds"] * 1e6, 2),
             "other_us": round(rest * 1e6, 2), "vector_bytes_per_even_site": vec_bytes,

@@ -276,8 +276,10 @@ __device__ __forceinline__ bool mx_halt(const MxState *st) { return st->done || 
 // Layout of the reduction scratch (red_partials) in the mixed CG: per-block
 // <p, Ap> partials from 0, the update's |r|^2 partials from kMxR2, the half
 // sweep's |Ap|^2 partials from kMxApAp, the fused update's second set of
-// |r|^2 partials from kMxR2b (it reads one set and writes the other)
-constexpr int kMxR2 = kMaxRedBlocks, kMxApAp = 2 * kMaxRedBlocks, kMxR2b = 3 * kMaxRedBlocks;
+// |r|^2 partials from kMxR2b (it reads one set and writes the other), the
+// 16-bit half sweep's Re <r, Ap> partials from kMxRAp
+constexpr int kMxR2 = kMaxRedBlocks, kMxApAp = 2 * kMaxRedBlocks, kMxR2b = 3 * kMaxRedBlocks,
+              kMxRAp = 4 * kMaxRedBlocks;
 
 // The reliable-update test of the iterated |r|^2 = r2 after itn
 // iterations (one thread): |r| against delta times the largest |r| since
@@ -350,6 +352,7 @@ struct DslashArgsLo {
   double *partials;
   unsigned *ticket;
   double *dot_out;      // RED == 2
+  const float2 *rdot = nullptr;  // RED == 4, 16-bit kernel: also Re <rdot, out> partials (kMxRAp)
   // output sites [k_lo, min(k_hi, nh)) of the parity (a domain's interior or
   // its intermediate slices); site k is stored at index k - out_off of out
   int k_lo = 0, k_hi = 0x7fffffff, out_off = 0;
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
   const size_t out_base = (size_t)A.po * nh;
   const float rho = A.L.long_scale / A.L.fat_scale;
   double dot = 0.0;
-  float fdot = 0.f, fdot2 = 0.f;
+  float fdot = 0.f, fdot2 = 0.f, fdot3 = 0.f;
   const int kend = min(nh, A.k_hi);
   for (int k = A.k_lo + blockIdx.x * blockDim.x + threadIdx.x; k < kend; k += gridDim.x * blockDim.x) {
     int x[4], lex;
@@ -565,6 +568,13 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
         fdot = fmaf(xsv[c].x, o[c].x, fmaf(xsv[c].y, o[c].y, fdot));
         fdot2 = fmaf(o[c].x, o[c].x, fmaf(o[c].y, o[c].y, fdot2));
       }
+      if (A.rdot != nullptr) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float2 r = __ldcg(A.rdot + (size_t)c * A.ostride + (k - A.out_off));
+          fdot3 = fmaf(r.x, o[c].x, fmaf(r.y, o[c].y, fdot3));
+        }
+      }
     } else if (RED) {
       float dd = 0.f;
 #pragma unroll
@@ -573,12 +583,13 @@ __global__ void __launch_bounds__(kBlock, 4) dslash_x2_kernel(const DslashArgsLo
     }
   }
   if (RED == 4) {
-    __shared__ double sh4[64];
-    double v[2] = {(double)fdot, (double)fdot2};
-    block_sum<2>(v, sh4);
+    __shared__ double sh4[96];
+    double v[3] = {(double)fdot, (double)fdot2, (double)fdot3};
+    block_sum<3>(v, sh4);
     if (threadIdx.x == 0) {
       A.partials[blockIdx.x] = v[0];
       A.partials[kMxApAp + blockIdx.x] = v[1];
+      if (A.rdot != nullptr) A.partials[kMxRAp + blockIdx.x] = v[2];
     }
   } else if (RED == 2) {
     double v[1] = {dot}, sm[1];
@@ -644,7 +655,8 @@ static int launch_lo(const DslashArgsLo &A, int) {
 //   which 1: ap = 4 m2 p - (2D)_{par,q} t      (out: FP32, hop -1, pAp)
 //   red 2: Re <p, Ap> summed into *dot_out (last-block reduction)
 //   red 4: per-block partials of <p, Ap> in partials[0 .. *blocks) and of
-//          |Ap|^2 from partials[kMxApAp]
+//          |Ap|^2 from partials[kMxApAp]; with A.rdot (16-bit links) also
+//          of Re <rdot, Ap> from partials[kMxRAp]
 template <int PREC, int NL>
 static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int *blocks) {
   constexpr int VP = VecPrec<PREC>::v;
@@ -664,9 +676,11 @@ static int sloppy_half(int which, const DslashArgsLo &A, int grid, int red, int 
 }
 
 // sloppy Schur: ap (FP32 [3][nh]) = 4 m2 p - (2D)(2D) p on parity par,
-// p and t in format prec.
+// p and t in format prec; rdot (FP32 [3][nh], 16-bit links and red 4 only)
+// adds the Re <rdot, ap> partials.
 int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void *p, void *t,
-             double m2, int red, const MxState *halt, double *dot_out, int *red_blocks) {
+             double m2, int red, const MxState *halt, double *dot_out, int *red_blocks,
+             const float2 *rdot = nullptr) {
   const Geom &geo = g->l->g;
   DslashArgsLo A;
   A.g = geo;
@@ -698,6 +712,7 @@ int schur_lo(const qexstag_links_s *g, int prec, int par, float2 *ap, const void
   A.sstride = geo.nh;
   A.out = ap;
   A.b = (float)(4.0 * m2);
+  A.rdot = rdot;
   if (prec == kF32)
     rc = g->nl == 8 ? sloppy_half<kF32, 8>(1, A, grid, red, red_blocks)
                     : sloppy_half<kF32, 4>(1, A, grid, red, red_blocks);
@@ -799,15 +814,20 @@ __global__ void __launch_bounds__(kBlock)
 //   partials at r2in, nr2 of them; nr2 = 0 right after the start or a
 //   reliable update, when r2 is the state's), then
 //   rs -= alpha ap; xs += alpha p_in; p_out = rs + beta p_in
-// with alpha = r2 / <p, Ap> and beta = (alpha^2 |Ap|^2 - r2) / r2 from the
-// half sweep's per-block partials (np of each).  Every block adds each set
-// of partials in the same order, so all take the same decisions.  In exact
-// arithmetic beta is CG's |r_new|^2 / |r|^2 (cg.nim:229-236), through
-// |r - alpha Ap|^2 = r2 - 2 alpha <r, Ap> + alpha^2 |Ap|^2 and <r, Ap> =
-// <p, Ap>; it is also the beta that makes the next direction A-orthogonal
-// to p, -<r_new, Ap> / <p, Ap>, under the same identity.  So p needs no
-// second pass over the sites; the exact |r_new|^2 is summed as well
-// (per-block partials at r2out) for the next update's alpha and test.  When the test stops the iteration nothing is
+// with alpha = r2 / <p, Ap> and beta from the half sweep's per-block
+// partials (np of each): with the partials of Re <r, Ap> (rap, the 16-bit
+// solve on one lattice), beta = -<r_new, Ap> / <p, Ap> = (alpha |Ap|^2 -
+// <r, Ap>) / <p, Ap>, the beta that makes the next direction A-orthogonal
+// to p for the operator actually applied; without them (rap null) beta =
+// (alpha^2 |Ap|^2 - r2) / r2, the same value once <r, Ap> = <p, Ap>.  In
+// exact arithmetic both are CG's |r_new|^2 / |r|^2 (cg.nim:229-236),
+// through |r - alpha Ap|^2 = r2 - 2 alpha <r, Ap> + alpha^2 |Ap|^2 and
+// <r, Ap> = <p, Ap>.  With 16-bit links the first form took 2828
+// iterations at 32^4 and delta 0.1 where the second took 2880.  Every block
+// adds each set of partials in the same order, so all take the same
+// decisions.  So p needs no second pass over the sites; the exact
+// |r_new|^2 is summed as well (per-block partials at r2out) for the next
+// update's alpha and test.  When the test stops the iteration nothing is
 // written: p_in, the direction a reliable update corrects, is intact in its
 // buffer (p_out is the other one), and the half sweeps of this iteration
 // were spent for nothing (once per reliable update).  Block 0 records the
@@ -817,7 +837,7 @@ template <int PREC>
 __global__ void __launch_bounds__(kBlock)
     mx_update_p_kernel(float2 *__restrict__ rs, float2 *__restrict__ xs, const float2 *__restrict__ ap,
                        const void *pin, void *pout, int n, MxState *st, const double *pap, const double *apap,
-                       int np, const double *r2in, int nr2, double *r2out, int par) {
+                       int np, const double *r2in, int nr2, double *r2out, int par, const double *rap = nullptr) {
   pdl_wait();
   if (mx_halt(st)) return;
   // the first site's operands are loaded before the sums of the partials,
@@ -837,14 +857,15 @@ __global__ void __launch_bounds__(kBlock)
   __shared__ float sh_ab[2];
   __shared__ int sh_go;
   {
-    double v3[3] = {0.0, 0.0, 0.0};
+    double v3[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = threadIdx.x; i < np; i += blockDim.x) {
       v3[0] += __ldcg(pap + i);
       v3[1] += __ldcg(apap + i);
+      if (rap != nullptr) v3[3] += __ldcg(rap + i);
     }
     for (int i = threadIdx.x; i < nr2; i += blockDim.x) v3[2] += __ldcg(r2in + i);
-    __shared__ double shp[96];
-    block_sum<3>(v3, shp);
+    __shared__ double shp[128];
+    block_sum<4>(v3, shp);
     if (threadIdx.x == 0) {
       const double s = v3[0], q = v3[1];
       const int itn = st->itc[par];
@@ -856,7 +877,7 @@ __global__ void __launch_bounds__(kBlock)
       }
       if (go) {
         const double alpha = r2 / s;
-        const double beta = (alpha * alpha * q - r2) / r2;
+        const double beta = rap != nullptr ? (alpha * q - v3[3]) / s : (alpha * alpha * q - r2) / r2;
         sh_ab[0] = (float)alpha;
         sh_ab[1] = (float)beta;
         if (blockIdx.x == 0) {
@@ -1058,11 +1079,13 @@ static int cg_mixed_t(qexstag_links_s *g, int par, double m2, CVecD b, VecD x, d
   auto batch = [&]() -> int {
     for (int i = 0; i < every; i++) {
       int np = 0;
-      int rc2 = schur_lo(g, PREC, par, ap, P[cur], pt, m2, 4, st, nullptr, &np);
+      constexpr bool hs = PREC == kF16;  // <r, Ap> partials from half sweep 2
+      int rc2 = schur_lo(g, PREC, par, ap, P[cur], pt, m2, 4, st, nullptr, &np, hs ? rs : nullptr);
       if (rc2) return rc2;
       launch_pdl(mx_update_p_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)P[cur],
                  P[cur ^ 1], nh, st, (const double *)red_partials(), (const double *)(red_partials() + kMxApAp),
-                 np, (const double *)R2[cur], fresh ? 0 : grid, R2[cur ^ 1], cur);
+                 np, (const double *)R2[cur], fresh ? 0 : grid, R2[cur ^ 1], cur,
+                 hs ? (const double *)(red_partials() + kMxRAp) : (const double *)nullptr);
       note_launch();
       cur ^= 1;
       fresh = false;
@@ -1392,7 +1415,7 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
     if ((rc2 = D.allreduce(D.ctx, val, 3))) return rc2;
     launch_pdl(mx_update_p_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)PI[cur],
                (void *)PI[cur ^ 1], n, st, (const double *)val, (const double *)(val + 1), 1,
-               (const double *)(val + 2), fresh ? 0 : 1, R2[cur ^ 1], cur);
+               (const double *)(val + 2), fresh ? 0 : 1, R2[cur ^ 1], cur, (const double *)nullptr);
     note_launch();
     QS_LAUNCH_CHECK();
     cur ^= 1;

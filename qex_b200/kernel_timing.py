@@ -3,6 +3,7 @@ and report HBM throughput against its compulsory bytes.
 
   python -m qex_b200.kernel_timing [--dims 32,32,32,32] [--naive]
                                    [--prec 0,1,2] [--nrep 20]
+  python -m qex_b200.kernel_timing --solve 2 [--delta 0.1]   (whole solves)
 
 Compulsory bytes per even site of one Schur application (each link read
 once per half sweep, each vector once; 12-real long links):
@@ -62,6 +63,8 @@ def main():
     ap.add_argument("--solve", type=int, default=-1,
                     help="instead: one warm-up and one timed solveEE (m=0.01, r2req 1e-20) "
                          "with this inner precision (0 FP64, 1 FP32, 2 16-bit)")
+    ap.add_argument("--delta", type=float, default=0.0,
+                    help="reliable-update threshold of the --solve runs (0: the library's default)")
     a = ap.parse_args()
     from . import fields as F
     from . import stag as S
@@ -78,14 +81,14 @@ def main():
         y = torch.zeros_like(b)
         out = {}
         for rep in ("warm", "timed"):
-            sp = S.SolverParams(r2req=1e-20, sloppySolve=a.solve)
+            sp = S.SolverParams(r2req=1e-20, sloppySolve=a.solve, delta=a.delta)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             s.solveEE(y, b, 0.01, sp)
             torch.cuda.synchronize()
             out[rep] = {"seconds": time.perf_counter() - t0, "iterations": sp.iterations,
                         "launches": sp.kernel_launches, "reliable_updates": sp.reliable_updates}
-        print(json.dumps({"dims": dims, "solve": a.solve, **out}))
+        print(json.dumps({"dims": dims, "solve": a.solve, "delta": a.delta, **out}))
         return
     res = time_schur(s, F.volume(dims) // 2, [int(v) for v in a.prec.split(",")], a.nrep)
     print(json.dumps({"dims": dims, "nlinks": s.nlinks, "recon12": s.recon12, "schur": res}))
