@@ -815,8 +815,8 @@ __global__ void __launch_bounds__(kBlock)
 //   reliable update, when r2 is the state's), then
 //   rs -= alpha ap; xs += alpha p_in; p_out = rs + beta p_in
 // with alpha = r2 / <p, Ap> and beta from the half sweep's per-block
-// partials (np of each): with the partials of Re <r, Ap> (rap, the 16-bit
-// solve on one lattice), beta = -<r_new, Ap> / <p, Ap> = (alpha |Ap|^2 -
+// partials (np of each): with the partials of Re <r, Ap> (rap: the 16-bit
+// solves, on one lattice or a domain), beta = -<r_new, Ap> / <p, Ap> = (alpha |Ap|^2 -
 // <r, Ap>) / <p, Ap>, the beta that makes the next direction A-orthogonal
 // to p for the operator actually applied; without them (rap null) beta =
 // (alpha^2 |Ap|^2 - r2) / r2, the same value once <r, Ap> = <p, Ap>.  In
@@ -1171,23 +1171,26 @@ __global__ void mxd_sum_kernel(const double *partials, int np, double *val) {
   if (threadIdx.x == 0) *val = v[0];
 }
 
-// the three sums of an iteration, in block order: <p, Ap> and |Ap|^2 (np
-// half-sweep partials each) and the previous update's |r|^2 (nr2 partials,
-// 0 when there is none) into val[0..2]
-__global__ void mxd_sum3_kernel(const double *pap, const double *apap, int np, const double *r2p, int nr2,
-                                double *val) {
-  __shared__ double sh[96];
-  double v[3] = {0.0, 0.0, 0.0};
+// the four sums of an iteration, in block order: <p, Ap>, |Ap|^2 and
+// Re <r, Ap> (np half-sweep partials each) and the previous update's |r|^2
+// (nr2 partials, 0 when there is none) into val[0..3] as <p, Ap>, |Ap|^2,
+// |r|^2, <r, Ap>
+__global__ void mxd_sum4_kernel(const double *pap, const double *apap, const double *rap, int np,
+                                const double *r2p, int nr2, double *val) {
+  __shared__ double sh[128];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
   for (int i = threadIdx.x; i < np; i += blockDim.x) {
     v[0] += __ldcg(pap + i);
     v[1] += __ldcg(apap + i);
+    v[3] += __ldcg(rap + i);
   }
   for (int i = threadIdx.x; i < nr2; i += blockDim.x) v[2] += __ldcg(r2p + i);
-  block_sum<3>(v, sh);
+  block_sum<4>(v, sh);
   if (threadIdx.x == 0) {
     val[0] = v[0];
     val[1] = v[1];
     val[2] = v[2];
+    val[3] = v[3];
   }
 }
 
@@ -1321,7 +1324,7 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
       (rc = ws.get(kSlotMx0 + 34, v32, &pap)) || (rc = ws.get(kSlotMx0 + 35, sizeof(uint4) * (size_t)nh, &pp)) ||
       (rc = ws.get(kSlotMx0 + 36, sizeof(uint4) * (size_t)nh, &pt)) ||
       (rc = ws.get(kSlotMx0 + 37, sizeof(MxState), &pst)) || (rc = ws.get(kSlotMx0 + 38, sizeof(double) * 4, &pval)) ||
-      (rc = ws.get(kSlotMx0 + 39, sizeof(double) * 4 * kMaxRedBlocks, &ppart)) ||
+      (rc = ws.get(kSlotMx0 + 39, sizeof(double) * 5 * kMaxRedBlocks, &ppart)) ||
       (rc = ws.get(kSlotMx0 + 40, sizeof(uint4) * (size_t)nh, &pp2)))
     return rc;
   double2 *r = (double2 *)pr, *ax = (double2 *)pax;
@@ -1393,10 +1396,11 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
   A2.b = (float)(4.0 * m2);
   A2.k_lo = D.even_lo;
   A2.k_hi = D.even_lo + n;
+  A2.rdot = rs;  // Re <r, Ap> partials (interior sites, as ap)
   // The three-kernel iteration of cg_mixed_t with one sum over the
   // processes per iteration: the ghost exchange of P[cur], the half sweeps,
-  // then <p, Ap>, |Ap|^2 and the previous update's |r|^2 summed in the
-  // domain and over the processes together, then the fused update.
+  // then <p, Ap>, |Ap|^2, <r, Ap> and the previous update's |r|^2 summed in
+  // the domain and over the processes together, then the fused update.
   int cur = 0;
   bool fresh = true;
   auto iteration = [&]() -> int {
@@ -1409,13 +1413,14 @@ int cg_mixed_domain(const MxDomain &D, double m2, const double2 *b, double2 *x, 
       return rc2;
     if ((rc2 = g->nl == 8 ? sloppy_half<PREC, 8>(1, A2, 0, 4, &np) : sloppy_half<PREC, 4>(1, A2, 0, 4, &np)))
       return rc2;
-    mxd_sum3_kernel<<<1, kBlock, 0, stream()>>>(part, part + kMxApAp, np, R2[cur], fresh ? 0 : grid, val);
+    mxd_sum4_kernel<<<1, kBlock, 0, stream()>>>(part, part + kMxApAp, part + kMxRAp, np, R2[cur],
+                                                fresh ? 0 : grid, val);
     note_launch();
     QS_LAUNCH_CHECK();
-    if ((rc2 = D.allreduce(D.ctx, val, 3))) return rc2;
+    if ((rc2 = D.allreduce(D.ctx, val, 4))) return rc2;
     launch_pdl(mx_update_p_kernel<VP>, grid, kBlock, rs, xs, (const float2 *)ap, (const void *)PI[cur],
                (void *)PI[cur ^ 1], n, st, (const double *)val, (const double *)(val + 1), 1,
-               (const double *)(val + 2), fresh ? 0 : 1, R2[cur ^ 1], cur, (const double *)nullptr);
+               (const double *)(val + 2), fresh ? 0 : 1, R2[cur ^ 1], cur, (const double *)(val + 3));
     note_launch();
     QS_LAUNCH_CHECK();
     cur ^= 1;
