@@ -656,6 +656,11 @@ def run_ours(args, dims):
                                    "GBps_no_reuse": round(v["GBps_no_reuse"], 1),
                                    "no_reuse_bytes_per_even_site": v["no_reuse_bytes_per_even_site"]}
                                for n, v in kt.items()}}
+    # the Schur call in SM cycles, so that boxes held at different clocks by
+    # the power cap compare (the call is too short to sample on its own)
+    sm_mhz = results[best]["clocks"].get("sm_mhz")
+    roof["cycles_per_call"] = round(k["seconds"] * sm_mhz * 1e6) if sm_mhz else None
+    roof["cycles_clock"] = "median SM clock sampled during the timed headline solves"
 
     # e2e: the same solve through the C ABI with host buffers in pinned
     # memory: per solve the library copies the source's even half in and
