@@ -1,8 +1,9 @@
 """ctypes wrapper of the CPU oracle (qexstag_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: used by tests/, the smoke check and the CPU
-baseline leg of bench.py, as the checker.  PARITY UNPINNED: see the header
-of qexstag_oracle.c.
+baseline leg of bench.py, as the checker.  Parity is pinned against QEX's
+logged solver output on the free HISQ field and otherwise by known answers:
+see the header of qexstag_oracle.c.
 
 Fields use the QEX V=1 host layout: complex128 (V, 3) colour vectors and
 (nlinks, V, 3, 3) link lists.

@@ -5,12 +5,16 @@
  * (qex_b200/csrc): tests, the smoke check and the CPU-baseline leg of the
  * benchmark may call it; the product path never does.
  *
- * PARITY UNPINNED.  QEX is written in Nim and no Nim compiler exists on the
- * build or GPU machines, so QEX's own stagD/CG cannot be run to produce
- * reference outputs, and QEX stores no golden vectors at the Dslash / CG /
- * force level (its reproducibility tests pin whole-HMC Hamiltonians that
- * depend on its RNG, SIMD layout and external integrator package).  This
- * restatement is instead pinned by analytic known answers, checked in
+ * PARITY PINNED AT THE SOLVER LEVEL, NOT ELEMENT BY ELEMENT.  QEX is written
+ * in Nim and no Nim compiler exists on the build or GPU machines, so QEX's
+ * own stagD/CG cannot be run to produce reference outputs, and QEX stores no
+ * golden vectors at the Dslash / CG / force level.  Its HISQ HMC regression
+ * logs (src/alphas/regression/) do record the first solves of a cold-start
+ * 8^3 x 16 trajectory: with the HISQ smearing of phased unit links, D and the
+ * full-lattice solve restated here, this oracle takes the same iteration
+ * counts (26, 26, 34) and ends at residuals of the same size
+ * (tests/test_oracle_qex_regression.py, fixture tests/golden/).  Element by
+ * element the restatement is pinned by analytic known answers, checked in
  * tests/test_oracle.py: the free-field spectrum 4(m^2 + sum_mu sin^2 p_mu)
  * with antiperiodic time, antihermiticity of the hopping term, gauge
  * covariance, the Schur identity, CG/multi-shift residuals and central finite
