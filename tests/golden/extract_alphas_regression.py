@@ -9,9 +9,11 @@ HISQ-smeared cold field: the ratio pseudofermion's heatbath
 (alphas.nim:722-745, D(-0.6)^-1 D(-0.005) eta) and the two terms of the
 initial fermion action (alphas.nim:694-707, D(-0.6)^-1 phi and
 D(-0.005)^-1 D(-0.6) hphi).  QEX prints each as
-"stagSolve: <iterations> <time> <rate> <r2/b2>".  This script reads the
-first three such lines and the run parameters of every log, checks that
-all logs agree, and writes them out.
+"stagSolve: <iterations> <time> <rate> <r2/b2>", then the Hamiltonian's
+parts ("kinetic: .. gauge: .. fermion: ..").  This script reads the first
+three such lines, the start-of-trajectory gauge and fermion actions and the
+run parameters of every log, checks that all logs agree, and writes them
+out.
 
   python tests/golden/extract_alphas_regression.py [QEX source root]
 """
@@ -36,6 +38,10 @@ def parse(log: Path):
         "action_r2req": float(re.search(r"minimum squared residual \(action CG solver\): (\S+)", text).group(1)),
         "naik": float(re.search(r"^naik: (\S+)", text, re.M).group(1)),
     }
+    # the Hamiltonian's parts at the start of the trajectory (alphas.nim:709-718)
+    h0 = re.search(r"^kinetic: (\S+) gauge: (\S+) fermion: (\S+)", text, re.M)
+    params["start_gauge_action"] = float(h0.group(2))
+    params["start_fermion_action"] = float(h0.group(3))
     solves = re.findall(r"^stagSolve: (\d+)\s+\S+\s+\S+\s+(\S+)", text, re.M)
     # logs of runs over several processes interleave identical lines of
     # every process: keep the first occurrence of each (iterations, r2)
@@ -55,6 +61,7 @@ def main():
     assert logs, f"no regression logs under {root}"
     runs = [(log, *parse(log)) for log in logs]
     params, solves = runs[0][1], runs[0][2]
+    actions = [p.pop("start_fermion_action") for _, p, _ in runs]
     for log, p, s in runs:
         assert p == params, (log, p)
         assert [x["iterations"] for x in s] == [x["iterations"] for x in solves], (log, s)
@@ -63,8 +70,12 @@ def main():
     for k, sv in enumerate(solves):
         r2s = [s[k]["r2_over_b2"] for _, _, s in runs]
         sv["r2_over_b2"] = [min(r2s), max(r2s)]
+    # S_F = (|psi|^2 + |hpsi|^2) / 2 after those solves (alphas.nim:694-707),
+    # equal across the logs up to summation order
+    params["start_fermion_action"] = [min(actions), max(actions)]
     out = {
-        "source": "QEX src/alphas/regression/*/*.log: the first three stagSolve lines of each run",
+        "source": "QEX src/alphas/regression/*/*.log: the first three stagSolve lines and the "
+                  "start-of-trajectory action of each run",
         "logs": [str(log.relative_to(root)) for log in logs],
         "params": params,
         "solves": [

@@ -22,7 +22,9 @@ rephase before smearing (alphas/extra/qexsmear.nim:90-98), both fat7 levels,
 projectU and the Naik term (9/8 and -1/24 times the phases on unit links),
 the phases and the antiperiodic boundary, D and its Schur operator with
 their normalisation, the solve's choice of preconditioning, and the CG's
-stopping rule.
+stopping rule.  The fermion action QEX logged after those solves (24323)
+lies within the spread of the oracle's over sources, which pins the
+Gaussian draws' normalisation and the action's.
 """
 import json
 from pathlib import Path
@@ -64,19 +66,16 @@ def test_free_hisq_links():
     assert np.allclose(lng, lng[:, :, 0, 0][:, :, None, None] * eye, atol=1e-15)
 
 
-@pytest.mark.parametrize("seed", [0, 1, 2])
-def test_start_of_trajectory_solves_match_qex_log(seed):
-    p = GOLDEN["params"]
-    dims = tuple(p["lattice"])
+def _start_of_trajectory(o, V, p, seed):
+    """The pseudofermion heatbath (alphas.nim:722-745) and the fermion action
+    (alphas.nim:694-707) on seeded Gaussians with unit variance in each real
+    component: ((iterations, r2/b2) of the three solves, S_F)."""
     m, mh, r2req = p["mass"], p["hasenbusch_mass"], p["action_r2req"]
-    V = int(np.prod(dims))
-    _, _, _, o = _free_hisq_oracle(dims)
     rng = np.random.default_rng(1000 + seed)
 
     def gaussian():
         return rng.standard_normal((V, 3)) + 1j * rng.standard_normal((V, 3))
 
-    # pseudofermion heatbath (alphas.nim:722-745)
     hpsi, psi = gaussian(), gaussian()
     phi, hphit, hphi = o.vec(), o.vec(), o.vec()
     o.D(phi, psi, -mh)
@@ -84,13 +83,37 @@ def test_start_of_trajectory_solves_match_qex_log(seed):
     runs = [o.solve(hphi, hphit, -mh, r2req)]
     phi[V // 2:] = 0
     hphi[V // 2:] = 0
-    # fermion action (alphas.nim:694-707)
     hpsit, x1, x2 = o.vec(), o.vec(), o.vec()
     o.D(hpsit, hphi, -mh)
     runs.append(o.solve(x1, phi, -mh, r2req))
     runs.append(o.solve(x2, hpsit, -m, r2req))
+    return runs, 0.5 * (np.vdot(x1, x1).real + np.vdot(x2, x2).real)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_start_of_trajectory_solves_match_qex_log(seed):
+    p = GOLDEN["params"]
+    dims = tuple(p["lattice"])
+    _, _, _, o = _free_hisq_oracle(dims)
+    runs, _ = _start_of_trajectory(o, int(np.prod(dims)), p, seed)
     for (its, r2), want in zip(runs, GOLDEN["solves"]):
         assert its == want["iterations"], (want["what"], its)
         lo, hi = want["r2_over_b2"]
         # the same size of final residual as QEX's (its sources differ)
-        assert r2 <= r2req and lo / 4 <= r2 <= hi * 4, (want["what"], r2, lo, hi)
+        assert r2 <= p["action_r2req"] and lo / 4 <= r2 <= hi * 4, (want["what"], r2, lo, hi)
+
+
+def test_start_of_trajectory_fermion_action_matches_qex_log():
+    """S_F = (|psi|^2 + |hpsi|^2)/2 after the three solves.  Over Gaussian
+    sources it spreads by about 165 (0.7 %) around 24600; QEX's one sample
+    is 24323.  A factor in the normalisation of the Gaussian draws (QEX's
+    randomComplexGaussian: unit variance in each real component) or of the
+    action would move it by 50 % or more, so the oracle's mean over four
+    sources must lie within 750 (4 standard deviations of the difference)."""
+    p = GOLDEN["params"]
+    dims = tuple(p["lattice"])
+    _, _, _, o = _free_hisq_oracle(dims)
+    actions = [_start_of_trajectory(o, int(np.prod(dims)), p, seed)[1] for seed in range(10, 14)]
+    qex = float(np.mean(p["start_fermion_action"]))
+    assert abs(np.mean(actions) - qex) <= 750.0, (actions, qex)
+    assert p["start_gauge_action"] == 0.0  # the cold configuration
