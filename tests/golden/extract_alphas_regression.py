@@ -55,8 +55,12 @@ def parse(log: Path):
     return params, first
 
 
-def main():
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+DEFAULT_ROOT = Path("/root/reference")
+FIXTURE = HERE / "qex_alphas_regression_8x8x8x16.json"
+
+
+def extract(root: Path = DEFAULT_ROOT) -> dict:
+    """The fixture's content, read from the logs under root."""
     logs = sorted((root / "src/alphas/regression").glob("*/*.log"))
     assert logs, f"no regression logs under {root}"
     runs = [(log, *parse(log)) for log in logs]
@@ -86,9 +90,14 @@ def main():
              **solves[2]},
         ],
     }
-    path = HERE / "qex_alphas_regression_8x8x8x16.json"
-    path.write_text(json.dumps(out, indent=1) + "\n")
-    print(path, [s["iterations"] for s in solves])
+    return out
+
+
+def main():
+    root = Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_ROOT
+    out = extract(root)
+    FIXTURE.write_text(json.dumps(out, indent=1) + "\n")
+    print(FIXTURE, [s["iterations"] for s in out["solves"]])
 
 
 if __name__ == "__main__":

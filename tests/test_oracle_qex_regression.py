@@ -117,3 +117,16 @@ def test_start_of_trajectory_fermion_action_matches_qex_log():
     qex = float(np.mean(p["start_fermion_action"]))
     assert abs(np.mean(actions) - qex) <= 750.0, (actions, qex)
     assert p["start_gauge_action"] == 0.0  # the cold configuration
+
+
+def test_fixture_is_what_the_logs_hold():
+    """The committed fixture equals a fresh extraction from QEX's logs, where
+    the QEX source tree is at hand (skipped elsewhere)."""
+    import importlib.util
+    path = Path(__file__).resolve().parent / "golden" / "extract_alphas_regression.py"
+    spec = importlib.util.spec_from_file_location("extract_alphas_regression", path)
+    ex = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ex)
+    if not (ex.DEFAULT_ROOT / "src/alphas/regression").is_dir():
+        pytest.skip("QEX source tree not present")
+    assert ex.extract() == GOLDEN
